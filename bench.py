@@ -1,0 +1,376 @@
+#!/usr/bin/env python
+"""Benchmark of the GRay2 geodesic hot path on B200.
+
+Workload (default): torus_rt_1024 -- a=0.998 Kerr-Schild, 17 deg camera at
+r=1000 M, 1024x1024 rays over +-20 M, RK4 with the reference step control
+(64 dumps of -31.25 M with 1000 substeps: affine parameter 0 -> -2000 M),
+radiative transfer at 4 frequencies through the analytic torus.  One bench
+step = one full render (icond + every dump interval of every ray).
+
+Metric: ray-steps/s = accepted RK4 steps summed over rays / time.
+  value       mixed-precision persistent kernel, inputs resident in HBM,
+              CUDA events on the launching stream, L2 flushed between steps
+  fp64        the plain FP64 kernel (one launch per dump) on the same render
+  e2e         the same metric through the C ABI with host buffers: render
+              plus the device-to-host copy of the final state every step
+  roofline    FP32 CUDA-core bound (the path has no dense contraction);
+              peak = FMA-loop microbenchmark measured in this run
+  cpu_baseline  the C oracle on the host cores, bounded ray sample
+
+--impl reference times the reference's CPU implementation of the path:
+the reference's OpenCL build cannot run here (no OpenCL platform, no lux
+runtime, and its analytic Kerr-Schild kernel does not compile as shipped),
+so its restatement in oracle/ (test/baseline infrastructure) is timed with
+every host thread on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): every rank renders its own copy of the workload
+(independent renders, weak scaling); the only collective is the max-over-
+ranks of the timed region.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from gray_b200 import configs, flops  # noqa: E402
+
+WORKLOADS = {"torus_rt_1024": configs.TORUS_RT_1024,
+             "kerr_small_64": configs.KERR_SMALL_64}
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+METRIC = "ray-steps/s"
+
+# DRAM bytes per launch of the dominant kernel from the committed ncu
+# capture (profiles/mixed_kernel_torus_rt.md), scaled to a full render.
+TRAFFIC = {}
+# Host-to-device bytes of one render through the C ABI: the render's table
+# entry (sizeof(MixedRender) in gray_b200/csrc/mixed_table.h); the camera
+# initial conditions are generated on the device.
+H2D_BYTES_PER_RENDER = 184
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="torus_rt_1024", choices=sorted(WORKLOADS))
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--side", type=int, default=0, help="override the camera side (small runs)")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ CPU side
+
+def cpu_rate(cfg, seconds, max_batches=10 ** 6):
+    """Oracle ray-steps/s on every host thread over a strided ray sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    n_rays = cfg["n_width"] * cfg["n_height"]
+    threads = os.cpu_count() or 1
+    batch = max(threads * 2, 16)
+    stride = 7919  # prime stride: rays from every part of the image
+    done_steps, done_rays, t_used, k = 0, 0, 0.0, 0
+    while t_used < seconds and k < max_batches:
+        rays = (np.arange(k * batch, (k + 1) * batch, dtype=np.int64) * stride) % n_rays
+        t0 = time.perf_counter()
+        _, _, steps = O.trace(cfg, rays, nthreads=threads)
+        t_used += time.perf_counter() - t0
+        done_steps += int(steps.sum())
+        done_rays += batch
+        k += 1
+    return done_steps / t_used, threads, done_rays, t_used
+
+
+def reference_arm(args, cfg, rank):
+    if rank != 0:
+        return
+    per_step = max(args.cpu_seconds / max(args.steps, 1), 1.0)
+    for _ in range(args.warmup):
+        cpu_rate(cfg, 0.0, max_batches=1)
+    rates, rays, secs = [], 0, 0.0
+    threads = 1
+    for _ in range(args.steps):
+        r, threads, n, s = cpu_rate(cfg, per_step)
+        rates.append(r)
+        rays += n
+        secs += s
+    value = float(np.mean(rates))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "ray-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "rays_per_render": cfg["n_width"] * cfg["n_height"],
+                   "sample": "strided rays", "precision": "fp64"},
+        "cpu_baseline": {"value": value, "unit": "ray-steps/s", "cores": threads,
+                         "kind": "port",
+                         "sample": "%d rays of %s (stride 7919), every dump interval, %.1f s"
+                                   % (rays, args.workload, secs)},
+        "e2e": {"value": value, "unit": "ray-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.th.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        load = [s for s in sm if mx and s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ GPU side
+
+def timed_renders(torch, render, k, flush):
+    """k renders; per render events around icond+evolve and around evolve
+    (the dominant kernel).  Returns (total_s, kernel_s)."""
+    evs = []
+    for _ in range(k):
+        flush.zero_()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        render.icond()
+        e1.record()
+        render.evolve_all(wait=False)
+        e2.record()
+        evs.append((e0, e1, e2))
+    torch.cuda.synchronize()
+    tot = sum(a.elapsed_time(c) for a, b, c in evs) * 1e-3
+    ker = sum(b.elapsed_time(c) for a, b, c in evs) * 1e-3
+    return tot, ker
+
+
+def max_over_ranks(torch, dist, x):
+    if dist is None:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(torch, dist):
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def ours_arm(args, cfg, rank, local_rank, world, dist):
+    import torch
+    from gray_b200 import api
+
+    torch.cuda.set_device(local_rank)
+    ctx = api.Context(local_rank)
+    # One created stream for the library's launches and torch's events (the
+    # legacy default stream has handle 0, which the C ABI reads as "use the
+    # context's own stream").
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    nf = len(cfg.get("nu", ()))
+    n_rays = cfg["n_width"] * cfg["n_height"]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    peak32 = ctx.measure_peak(api.PREC_MIXED)
+    peak64 = ctx.measure_peak(api.PREC_FP64)
+
+    # ---- mixed (headline)
+    rm = ctx.render(dict(cfg, precision=api.PREC_MIXED))
+    for _ in range(args.warmup):
+        rm.run()
+    steps_per_render = rm.steps()
+    barrier(torch, dist)
+    clk = ClockSampler(local_rank)
+    clk.start()
+    tot, ker = timed_renders(torch, rm, args.steps, flush)
+    clocks = clk.stop()
+    barrier(torch, dist)
+    tot = max_over_ranks(torch, dist, tot)
+    ker = max_over_ranks(torch, dist, ker)
+    value = world * steps_per_render * args.steps / tot
+    mixed_state, mixed_info = rm.state(api.LAYOUT_SOA)
+
+    flop_step = flops.mixed_per_step(nf)
+    achieved = steps_per_render * flop_step / (ker / args.steps) / 1e12
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak32 / 1e12,
+                "unit": "TFLOP/s", "frac": achieved * 1e12 / peak32,
+                "traffic": TRAFFIC.get(args.workload),
+                "peak_source": "FMA-loop microbenchmark in this run (best of scalar and f32x2 FFMA)",
+                "flop_per_ray_step": flop_step,
+                "kernel": "mixed_kernel<%d>" % nf}
+
+    # ---- plain FP64 on the same render
+    fp64 = None
+    if not args.no_fp64:
+        r64 = ctx.render(dict(cfg, precision=api.PREC_FP64))
+        r64.run()  # warm-up
+        s64 = r64.steps()
+        barrier(torch, dist)
+        t64, k64 = timed_renders(torch, r64, args.fp64_steps, flush)
+        barrier(torch, dist)
+        t64 = max_over_ranks(torch, dist, t64)
+        k64 = max_over_ranks(torch, dist, k64)
+        v64 = world * s64 * args.fp64_steps / t64
+        st64, _ = r64.state(api.LAYOUT_SOA)
+        img = {}
+        for i in range(nf):
+            ref = st64[8 + i]
+            img["nu%g" % cfg["nu"][i]] = float(np.linalg.norm(mixed_state[8 + i] - ref) /
+                                               np.linalg.norm(ref))
+        pos = float(np.linalg.norm(mixed_state[1:4] - st64[1:4]) / np.linalg.norm(st64[1:4]))
+        a64 = s64 * flops.fp64_per_step(nf) / (k64 / args.fp64_steps) / 1e12
+        fp64 = {"value": v64, "unit": "ray-steps/s",
+                "ms_per_step": 1e3 * t64 / args.fp64_steps,
+                "ray_steps_per_render": s64,
+                "mixed_over_fp64": value / v64,
+                "image_rel_l2_err": img, "end_position_rel_l2_err": pos,
+                "roofline": {"bound": "fp64", "achieved": a64, "peak": peak64 / 1e12,
+                             "unit": "TFLOP/s", "frac": a64 * 1e12 / peak64,
+                             "flop_per_ray_step": flops.fp64_per_step(nf)},
+                "launches_per_render": 1 + int(cfg["n_dump"])}
+        r64.close()
+
+    # ---- end to end: render + device-to-host copy of the state, host buffers
+    host = torch.empty((8 + 2 * nf) * n_rays, dtype=torch.float64, pin_memory=True).numpy()
+    host = host.reshape(8 + 2 * nf, n_rays)
+    hinfo = torch.empty(n_rays, dtype=torch.float64, pin_memory=True).numpy()
+    rm.run()
+    rm.state(api.LAYOUT_SOA, out=host, info_out=hinfo)
+    barrier(torch, dist)
+    e2e_t = 0.0
+    for _ in range(args.e2e_steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rm.run(wait=False)
+        rm.state(api.LAYOUT_SOA, out=host, info_out=hinfo)  # synchronous d2h
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_t += e0.elapsed_time(e1) * 1e-3
+    barrier(torch, dist)
+    e2e_t = max_over_ranks(torch, dist, e2e_t)
+    e2e = {"value": world * steps_per_render * args.e2e_steps / e2e_t, "unit": "ray-steps/s",
+           "h2d_bytes_per_step": H2D_BYTES_PER_RENDER,
+           "d2h_bytes_per_step": int(host.nbytes + hinfo.nbytes)}
+    rm.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, cores, rays, secs = cpu_rate(cfg, args.cpu_seconds)
+        cpu = {"value": rate, "unit": "ray-steps/s", "cores": cores, "kind": "port",
+               "sample": "%d rays of %s (stride 7919), every dump interval, %.1f s"
+                         % (rays, args.workload, secs)}
+
+    ctx.close()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "ray-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64-islands", "data": "synthetic",
+        "config": {"workload": args.workload, "rays_per_render": n_rays,
+                   "renders_per_gpu_per_step": 1, "n_freq": nf, "a_spin": cfg["a_spin"],
+                   "i_obs": cfg["i_obs"], "affine_range": cfg["dt_dump"] * cfg["n_dump"],
+                   "n_sub": cfg["n_sub"], "ray_steps_per_render": steps_per_render,
+                   "precision": "mixed", "l2": "flushed (256 MiB write) between steps",
+                   "parallelism": "independent renders per GPU" if world > 1 else "single GPU"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": 2 * args.steps, "clocks": clocks, "fp64": fp64,
+        "peaks_measured_tflops": {"fp32": peak32 / 1e12, "fp64": peak64 / 1e12},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    cfg = dict(WORKLOADS[args.workload])
+    if args.side:
+        cfg = configs.scaled(cfg, args.side)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, cfg, rank)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as D
+        torch.cuda.set_device(local_rank)
+        D.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                             device_id=torch.device("cuda", local_rank))
+        dist = D
+    try:
+        ours_arm(args, cfg, rank, local_rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

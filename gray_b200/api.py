@@ -1,0 +1,285 @@
+"""Python view of the C ABI in include/gray_cuda.h (ctypes, no torch types).
+
+This mirrors the lux-job surface of the reference (sim/gray.opts,
+sim/Kerr.opts, sim/infcam.opts, sim-org/setup.opts, sim-org/param.opts):
+a RenderDesc carries the same run-time parameter names, and Context.run()
+does what sim-org/gray.c:_exec does for the analytic spacetime (icond, then
+one evolve per dump interval) on the GPU.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libgray_cuda.so")
+MAX_FREQ = 8
+
+OK, EINVAL, ENOMEM, ECUDA, ENODEV, EBUDGET, ETIMEOUT, ENOTFOUND, ESTATE, ESIZE = (
+    0, -1, -2, -3, -4, -5, -6, -7, -8, -9)
+PREC_FP64, PREC_MIXED = 0, 1
+ST_KERR, ST_NUMERICAL = 0, 1
+FLOW_NONE, FLOW_TORUS = 0, 1
+TERM_EPS, TERM_RPLUS = 0, 1
+LAYOUT_SOA, LAYOUT_AOS = 0, 1
+
+# Every symbol include/gray_cuda.h declares.
+EXPORTS = [
+    "gray_strerror", "gray_abi_version", "gray_create", "gray_destroy",
+    "gray_set_stream", "gray_sync", "gray_hbm_used", "gray_render_create",
+    "gray_render_destroy", "gray_icond", "gray_evolve", "gray_run", "gray_evolve_all",
+    "gray_read_state", "gray_write_state", "gray_read_kdown", "gray_ray_steps",
+    "gray_load_spacetime", "gray_load_spacetime_interleaved",
+    "gray_make_boosted_ks", "gray_swap_levels", "gray_measure_peak",
+]
+
+
+class GrayError(RuntimeError):
+    def __init__(self, status, what):
+        super().__init__("%s: %s (%d)" % (what, strerror(status), status))
+        self.status = status
+
+
+class RenderDesc(ctypes.Structure):
+    _fields_ = [
+        ("m_bh", ctypes.c_double), ("a_spin", ctypes.c_double),
+        ("w_img", ctypes.c_double), ("h_img", ctypes.c_double),
+        ("r_obs", ctypes.c_double), ("i_obs", ctypes.c_double),
+        ("j_obs", ctypes.c_double),
+        ("n_width", ctypes.c_uint64), ("n_height", ctypes.c_uint64),
+        ("t_init", ctypes.c_double), ("dt_dump", ctypes.c_double),
+        ("n_sub", ctypes.c_uint64), ("n_dump", ctypes.c_uint64),
+        ("term", ctypes.c_int32),
+        ("n_freq", ctypes.c_int32), ("nu", ctypes.c_double * MAX_FREQ),
+        ("flow", ctypes.c_int32),
+        ("torus_n0", ctypes.c_double), ("torus_kappa", ctypes.c_double),
+        ("torus_hr", ctypes.c_double),
+        ("spacetime", ctypes.c_int32), ("precision", ctypes.c_int32),
+    ]
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+        ("box", ctypes.c_float * 8),
+        ("bug_gzz", ctypes.c_int32), ("physics", ctypes.c_int32),
+    ]
+
+
+# Reference defaults (sim/gray.opts, sim/Kerr.opts, sim/infcam.opts,
+# sim-org/setup.opts).
+DEFAULTS = dict(m_bh=4e6, a_spin=0.0, w_img=64.0, h_img=64.0, r_obs=1024.0,
+                i_obs=60.0, j_obs=0.0, n_width=512, n_height=512, t_init=0.0,
+                dt_dump=-32.0, n_sub=1024, n_dump=64, term=TERM_EPS, nu=(),
+                flow=None, torus_n0=1.0, torus_kappa=1.0, torus_hr=0.3,
+                spacetime=ST_KERR, precision=PREC_FP64)
+
+
+def make_desc(cfg):
+    c = dict(DEFAULTS)
+    c.update(cfg)
+    d = RenderDesc()
+    for k in ("m_bh", "a_spin", "w_img", "h_img", "r_obs", "i_obs", "j_obs",
+              "t_init", "dt_dump", "torus_n0", "torus_kappa", "torus_hr"):
+        setattr(d, k, float(c[k]))
+    for k in ("n_width", "n_height", "n_sub", "n_dump", "term", "spacetime", "precision"):
+        setattr(d, k, int(c[k]))
+    nu = list(c["nu"])
+    if len(nu) > MAX_FREQ:
+        raise ValueError("at most %d frequencies" % MAX_FREQ)
+    d.n_freq = len(nu)
+    for i, v in enumerate(nu):
+        d.nu[i] = float(v)
+    flow = c["flow"]
+    d.flow = int(flow) if flow is not None else (FLOW_TORUS if nu else FLOW_NONE)
+    return d
+
+
+_lib = None
+
+
+def lib():
+    """Load libgray_cuda.so; raise loudly when it is missing (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                "libgray_cuda.so is not built (%s); run __graft_entry__.build()" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER
+        vp, i, sz, d, u64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_double, ctypes.c_uint64
+        L.gray_strerror.restype = ctypes.c_char_p
+        L.gray_strerror.argtypes = [i]
+        L.gray_abi_version.restype = i
+        L.gray_create.restype = vp
+        L.gray_create.argtypes = [i, sz, P(i)]
+        L.gray_destroy.argtypes = [vp]
+        L.gray_destroy.restype = None
+        L.gray_set_stream.argtypes = [vp, vp]
+        L.gray_sync.argtypes = [vp]
+        L.gray_hbm_used.restype = sz
+        L.gray_hbm_used.argtypes = [vp]
+        L.gray_render_create.argtypes = [vp, P(RenderDesc), P(i)]
+        L.gray_render_destroy.argtypes = [vp, i]
+        L.gray_icond.argtypes = [vp, i]
+        L.gray_evolve.argtypes = [vp, i, d, d, u64, P(d)]
+        L.gray_run.argtypes = [vp, i, P(d)]
+        L.gray_evolve_all.argtypes = [vp, i, P(d)]
+        L.gray_read_state.argtypes = [vp, i, vp, sz, vp, sz, i]
+        L.gray_write_state.argtypes = [vp, i, vp, sz, i]
+        L.gray_read_kdown.argtypes = [vp, i, vp, sz]
+        L.gray_ray_steps.argtypes = [vp, i, P(u64)]
+        L.gray_load_spacetime.argtypes = [vp, P(GridDesc), P(ctypes.c_void_p), i]
+        L.gray_load_spacetime_interleaved.argtypes = [vp, P(GridDesc), vp, i]
+        L.gray_make_boosted_ks.argtypes = [vp, P(GridDesc), d, d, i, d, i]
+        L.gray_swap_levels.argtypes = [vp]
+        L.gray_measure_peak.argtypes = [vp, i, P(d)]
+        _lib = L
+    return _lib
+
+
+def strerror(status):
+    return lib().gray_strerror(status).decode()
+
+
+def _ck(status, what):
+    if status != OK:
+        raise GrayError(status, what)
+
+
+def make_grid(n, lo, hi, t1=0.0, t2=0.0, bug_gzz=False, physics=False):
+    g = GridDesc()
+    g.nx, g.ny, g.nz = (n, n, n) if isinstance(n, int) else n
+    lo3 = (lo,) * 3 if not hasattr(lo, "__len__") else lo
+    hi3 = (hi,) * 3 if not hasattr(hi, "__len__") else hi
+    box = [t1, lo3[0], lo3[1], lo3[2], t2, hi3[0], hi3[1], hi3[2]]
+    for k in range(8):
+        g.box[k] = box[k]
+    g.bug_gzz = int(bug_gzz)
+    g.physics = int(physics)
+    return g
+
+
+class Render:
+    def __init__(self, ctx, cfg):
+        self.ctx = ctx
+        self.desc = make_desc(cfg)
+        rid = ctypes.c_int(0)
+        _ck(lib().gray_render_create(ctx.h, ctypes.byref(self.desc), ctypes.byref(rid)),
+            "gray_render_create")
+        self.id = rid.value
+        self.n_rays = self.desc.n_width * self.desc.n_height
+        self.n_data = 8 + 2 * self.desc.n_freq
+
+    def icond(self):
+        _ck(lib().gray_icond(self.ctx.h, self.id), "gray_icond")
+
+    def evolve(self, t, target, n_sub=None, wait=True):
+        ns = ctypes.c_double(0.0)
+        n_sub = self.desc.n_sub if n_sub is None else n_sub
+        _ck(lib().gray_evolve(self.ctx.h, self.id, t, target, n_sub,
+                              ctypes.byref(ns) if wait else None), "gray_evolve")
+        return ns.value
+
+    def run(self, wait=True):
+        ns = ctypes.c_double(0.0)
+        _ck(lib().gray_run(self.ctx.h, self.id, ctypes.byref(ns) if wait else None),
+            "gray_run")
+        return ns.value
+
+    def evolve_all(self, wait=True):
+        ns = ctypes.c_double(0.0)
+        _ck(lib().gray_evolve_all(self.ctx.h, self.id, ctypes.byref(ns) if wait else None),
+            "gray_evolve_all")
+        return ns.value
+
+    def state(self, layout=LAYOUT_SOA, out=None, info_out=None):
+        if out is None:
+            shape = (self.n_data, self.n_rays) if layout == LAYOUT_SOA else (self.n_rays, self.n_data)
+            out = np.empty(shape, dtype=np.float64)
+        if info_out is None:
+            info_out = np.empty(self.n_rays, dtype=np.float64)
+        _ck(lib().gray_read_state(self.ctx.h, self.id, out.ctypes.data, out.nbytes,
+                                  info_out.ctypes.data, info_out.nbytes, layout),
+            "gray_read_state")
+        return out, info_out
+
+    def write_state(self, data, layout=LAYOUT_SOA):
+        data = np.ascontiguousarray(data, dtype=np.float64)
+        _ck(lib().gray_write_state(self.ctx.h, self.id, data.ctypes.data, data.nbytes, layout),
+            "gray_write_state")
+
+    def kdown(self):
+        k = np.empty((4, self.n_rays), dtype=np.float64)
+        _ck(lib().gray_read_kdown(self.ctx.h, self.id, k.ctypes.data, k.nbytes), "gray_read_kdown")
+        return k
+
+    def steps(self):
+        v = ctypes.c_uint64(0)
+        _ck(lib().gray_ray_steps(self.ctx.h, self.id, ctypes.byref(v)), "gray_ray_steps")
+        return v.value
+
+    def close(self):
+        if self.id:
+            lib().gray_render_destroy(self.ctx.h, self.id)
+            self.id = 0
+
+
+class Context:
+    """One CUDA device; owns every device allocation (gray_create)."""
+
+    def __init__(self, device=0, hbm_budget=0):
+        st = ctypes.c_int(0)
+        h = lib().gray_create(device, hbm_budget, ctypes.byref(st))
+        if not h:
+            raise GrayError(st.value, "gray_create")
+        self.h = h
+
+    def render(self, cfg):
+        return Render(self, cfg)
+
+    def set_stream(self, stream_ptr):
+        _ck(lib().gray_set_stream(self.h, stream_ptr), "gray_set_stream")
+
+    def sync(self):
+        _ck(lib().gray_sync(self.h), "gray_sync")
+
+    def hbm_used(self):
+        return lib().gray_hbm_used(self.h)
+
+    def load_spacetime(self, grid, fields, level):
+        """fields: [nz, ny, nx, 51] float32 array (interleaved) or a list of
+        51 [nz, ny, nx] arrays in io.c order."""
+        if isinstance(fields, np.ndarray):
+            f = np.ascontiguousarray(fields, dtype=np.float32)
+            _ck(lib().gray_load_spacetime_interleaved(self.h, ctypes.byref(grid),
+                                                      f.ctypes.data, level),
+                "gray_load_spacetime_interleaved")
+        else:
+            arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in fields]
+            ptrs = (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+            _ck(lib().gray_load_spacetime(self.h, ctypes.byref(grid), ptrs, level),
+                "gray_load_spacetime")
+
+    def make_boosted_ks(self, grid, a, v, axis, t, level):
+        _ck(lib().gray_make_boosted_ks(self.h, ctypes.byref(grid), a, v, axis, t, level),
+            "gray_make_boosted_ks")
+
+    def measure_peak(self, precision):
+        v = ctypes.c_double(0.0)
+        _ck(lib().gray_measure_peak(self.h, precision, ctypes.byref(v)), "gray_measure_peak")
+        return v.value
+
+    def swap_levels(self):
+        _ck(lib().gray_swap_levels(self.h), "gray_swap_levels")
+
+    def close(self):
+        if self.h:
+            lib().gray_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -1,0 +1,34 @@
+"""Named workloads of the geodesic hot path, with their sizes.
+
+kerr_small_64   a=0.9 Kerr-Schild, camera r=1000 M at 60 deg, 64x64 rays over
+                +-20 M, RK4 to affine parameter -2000 M (64 dumps of -31.25 M,
+                1000 substeps each, i.e. a 1/32 M step cap), FP64, no transfer.
+torus_rt_1024   a=0.998, 17 deg, 1024x1024 rays over +-20 M at r=1000 M, same
+                step control, transfer at nu = 1, 2, 4, 8 through the analytic
+                power-law torus; kappa is frozen so that tau(nu=1) = 1 along
+                the central ray (ray 512*1024+512).
+numerical_128   128^3 FP32 boosted Kerr-Schild grid (a=0.7, v=0.3 along x) on
+                [-40, 40]^3 with the n=3 fisheye map, levels t=0 and t=10 M;
+                512x512 camera at r=200 M, 45 deg, mixed precision.
+"""
+TORUS_KAPPA = 125.8988  # 1 / tau(nu=1) of the central ray with kappa = 1
+
+KERR_SMALL_64 = dict(
+    a_spin=0.9, w_img=40.0, h_img=40.0, r_obs=1000.0, i_obs=60.0, j_obs=0.0,
+    n_width=64, n_height=64, t_init=0.0, dt_dump=-31.25, n_sub=1000, n_dump=64,
+    nu=(),
+)
+
+TORUS_RT_1024 = dict(
+    a_spin=0.998, w_img=40.0, h_img=40.0, r_obs=1000.0, i_obs=17.0, j_obs=0.0,
+    n_width=1024, n_height=1024, t_init=0.0, dt_dump=-31.25, n_sub=1000, n_dump=64,
+    nu=(1.0, 2.0, 4.0, 8.0), torus_n0=1.0, torus_kappa=TORUS_KAPPA, torus_hr=0.3,
+)
+
+
+def scaled(cfg, side):
+    """The same workload on a side x side camera (parity-test sizes)."""
+    c = dict(cfg)
+    c["n_width"] = side
+    c["n_height"] = side
+    return c

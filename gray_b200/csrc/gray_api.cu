@@ -1,0 +1,885 @@
+/*
+ * C ABI of libgray_cuda (include/gray_cuda.h): contexts, renders, device
+ * memory under an HBM budget, and the launch sequence of the reference's
+ * host glue (sim-org/icond.c, evolve.c, gray.c:243-294, io.c:39-72).
+ */
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "gray_internal.h"
+#include "mixed_table.h"
+
+struct Render {
+	gray_render_desc desc;
+	RenderParams p;
+	double *d_data = nullptr;
+	double *d_info = nullptr;
+	unsigned long long *d_steps = nullptr;
+	unsigned int *d_queue = nullptr;
+	MixedRender *d_table = nullptr;       /* one-entry table for gray_run */
+	unsigned long long *d_prefix = nullptr;
+	size_t bytes = 0;
+	bool has_state = false;
+};
+
+struct Grid {
+	gray_grid_desc desc;
+	bool loaded[2] = {false, false};
+	float *lvl[2] = {nullptr, nullptr};
+	double *nodes[3] = {nullptr, nullptr, nullptr};
+	float *nodes_f[3] = {nullptr, nullptr, nullptr};
+	size_t bytes = 0;
+	GridParams gp;
+};
+
+struct gray_ctx {
+	int device = 0;
+	size_t budget = 0;
+	size_t used = 0;
+	int sms = 0;
+	cudaStream_t own = nullptr;
+	cudaStream_t stream = nullptr;
+	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+	std::map<int, Render *> renders;
+	int next_id = 1;
+	Grid *grid = nullptr;
+	int evolve64_block = 128;
+	MixedLaunch mixed = {256, 0, 0};
+};
+
+namespace {
+
+int
+from_cuda(cudaError_t e)
+{
+	if(e == cudaSuccess)
+		return GRAY_OK;
+	if(e == cudaErrorMemoryAllocation)
+		return GRAY_ENOMEM;
+	return GRAY_ECUDA;
+}
+
+#define CK(call)                                   \
+	do {                                           \
+		cudaError_t e_ = (call);                   \
+		if(e_ != cudaSuccess)                      \
+			return from_cuda(e_);                  \
+	} while(0)
+
+int
+dalloc(gray_ctx *c, void **p, size_t bytes)
+{
+	if(c->used + bytes > c->budget)
+		return GRAY_EBUDGET;
+	cudaError_t e = cudaMalloc(p, bytes);
+	if(e != cudaSuccess) {
+		*p = nullptr;
+		cudaGetLastError();
+		return GRAY_ENOMEM;
+	}
+	c->used += bytes;
+	return GRAY_OK;
+}
+
+void
+dfree(gray_ctx *c, void *p, size_t bytes)
+{
+	if(p) {
+		cudaFree(p);
+		c->used -= bytes;
+	}
+}
+
+Render *
+find(gray_ctx *c, int id)
+{
+	if(!c)
+		return nullptr;
+	auto it = c->renders.find(id);
+	return it == c->renders.end() ? nullptr : it->second;
+}
+
+/* Bardeen-Press-Teukolsky prograde ISCO (M = 1) */
+double
+risco_of(double a)
+{
+	double z1 = 1.0 + cbrt(1.0 - a * a) * (cbrt(1.0 + a) + cbrt(1.0 - a));
+	double z2 = sqrt(3.0 * a * a + z1 * z1);
+	return 3.0 + z2 - sqrt((3.0 - z1) * (3.0 + z1 + 2.0 * z2));
+}
+
+int
+check_desc(const gray_render_desc *d)
+{
+	if(!d)
+		return GRAY_EINVAL;
+	if(!(d->a_spin > -1.0 && d->a_spin < 1.0))
+		return GRAY_EINVAL;
+	if(d->n_width == 0 || d->n_height == 0 || d->n_sub == 0)
+		return GRAY_EINVAL;
+	if(d->n_width > (1u << 20) || d->n_height > (1u << 20))
+		return GRAY_EINVAL;
+	if((uint64_t)d->n_width * d->n_height > (1ull << 31))
+		return GRAY_EINVAL;
+	if(d->n_sub > (uint64_t)INT32_MAX)
+		return GRAY_EINVAL;
+	if(d->n_freq < 0 || d->n_freq > GRAY_MAX_FREQ)
+		return GRAY_EINVAL;
+	if(d->flow != GRAY_FLOW_NONE && d->flow != GRAY_FLOW_TORUS)
+		return GRAY_EINVAL;
+	if(d->term != GRAY_TERM_EPS && d->term != GRAY_TERM_RPLUS)
+		return GRAY_EINVAL;
+	if(d->precision != GRAY_PREC_FP64 && d->precision != GRAY_PREC_MIXED)
+		return GRAY_EINVAL;
+	if(d->spacetime != GRAY_ST_KERR && d->spacetime != GRAY_ST_NUMERICAL)
+		return GRAY_EINVAL;
+	if(d->spacetime == GRAY_ST_NUMERICAL && d->n_freq != 0)
+		return GRAY_EINVAL; /* dyst transfer needs the GRMHD flow: not built */
+	for(int i = 0; i < d->n_freq; ++i)
+		if(!(d->nu[i] > 0.0))
+			return GRAY_EINVAL;
+	if(!std::isfinite(d->dt_dump) || !std::isfinite(d->t_init))
+		return GRAY_EINVAL;
+	return GRAY_OK;
+}
+
+void
+make_params(const gray_render_desc *d, RenderParams *p)
+{
+	memset(p, 0, sizeof(*p));
+	p->a  = d->a_spin;
+	p->aa = d->a_spin * d->a_spin;
+	p->rp = 1.0 + sqrt(1.0 - d->a_spin * d->a_spin);
+	p->risco = risco_of(d->a_spin);
+	p->eps_stop = d->term == GRAY_TERM_RPLUS ? 0.01 * p->rp : 0.01;
+	const double deg2rad = 3.14159265358979323846264338327950288 / 180.0;
+	p->ci = cos(deg2rad * d->i_obs);
+	p->si = sin(deg2rad * d->i_obs);
+	p->cj = cos(deg2rad * d->j_obs);
+	p->sj = sin(deg2rad * d->j_obs);
+	p->w_img = d->w_img;
+	p->h_img = d->h_img;
+	p->r_obs = d->r_obs;
+	p->w_rays = (long long)d->n_width;
+	p->h_rays = (long long)d->n_height;
+	p->n_rays = p->w_rays * p->h_rays;
+	p->spacetime = d->spacetime;
+	p->flow = d->n_freq > 0 ? d->flow : GRAY_FLOW_NONE;
+	p->n_freq = d->n_freq;
+	p->n_data = 8 + 2 * d->n_freq;
+	p->torus_n0 = d->torus_n0;
+	p->torus_kappa = d->torus_kappa;
+	p->torus_hr = d->torus_hr;
+	for(int i = 0; i < d->n_freq; ++i) {
+		p->nupow[i]  = pow(d->nu[i], -0.7);
+		p->nuinv2[i] = 1.0 / (d->nu[i] * d->nu[i]);
+		p->nupow_f[i]  = (float)p->nupow[i];
+		p->nuinv2_f[i] = (float)p->nuinv2[i];
+	}
+}
+
+int
+timed_begin(gray_ctx *c)
+{
+	CK(cudaEventRecord(c->ev0, c->stream));
+	return GRAY_OK;
+}
+
+int
+timed_end(gray_ctx *c, double *ns)
+{
+	CK(cudaEventRecord(c->ev1, c->stream));
+	if(ns) {
+		CK(cudaEventSynchronize(c->ev1));
+		float ms = 0.0f;
+		CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+		*ns = (double)ms * 1e6;
+	}
+	return GRAY_OK;
+}
+
+int
+grid_ready(gray_ctx *c)
+{
+	if(!c->grid || !c->grid->loaded[0])
+		return 0;
+	if(!c->grid->gp.single && !c->grid->loaded[1])
+		return 0;
+	return 1;
+}
+
+} /* namespace */
+
+/* ------------------------------------------------------------------------ */
+
+extern "C" const char *
+gray_strerror(int s)
+{
+	switch(s) {
+	case GRAY_OK:        return "success";
+	case GRAY_EINVAL:    return "invalid argument or configuration";
+	case GRAY_ENOMEM:    return "out of memory";
+	case GRAY_ECUDA:     return "CUDA runtime error";
+	case GRAY_ENODEV:    return "no usable CUDA device";
+	case GRAY_EBUDGET:   return "request exceeds the HBM budget";
+	case GRAY_ETIMEOUT:  return "bounded device wait timed out";
+	case GRAY_ENOTFOUND: return "unknown render or request id";
+	case GRAY_ESTATE:    return "call out of order";
+	case GRAY_ESIZE:     return "buffer size mismatch";
+	default:             return "unknown status";
+	}
+}
+
+extern "C" int
+gray_abi_version(void)
+{
+	return GRAY_ABI_VERSION;
+}
+
+extern "C" gray_ctx *
+gray_create(int device, size_t hbm_budget, int *status)
+{
+	int st = GRAY_OK, n = 0;
+	gray_ctx *c = nullptr;
+	cudaDeviceProp prop;
+	size_t fr = 0, tot = 0;
+
+	if(cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+		cudaGetLastError();
+		st = GRAY_ENODEV;
+		goto out;
+	}
+	if(cudaSetDevice(device) != cudaSuccess ||
+	   cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+		st = GRAY_ENODEV;
+		goto out;
+	}
+	if(prop.major < 10) { /* built for sm_100a only */
+		st = GRAY_ENODEV;
+		goto out;
+	}
+	c = new(std::nothrow) gray_ctx;
+	if(!c) {
+		st = GRAY_ENOMEM;
+		goto out;
+	}
+	c->device = device;
+	c->sms = prop.multiProcessorCount;
+	if(cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+		st = GRAY_ECUDA;
+		goto fail;
+	}
+	c->budget = hbm_budget ? hbm_budget : (size_t)(0.9 * (double)fr);
+	if(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
+	   cudaEventCreate(&c->ev0) != cudaSuccess ||
+	   cudaEventCreate(&c->ev1) != cudaSuccess) {
+		st = GRAY_ECUDA;
+		goto fail;
+	}
+	c->stream = c->own;
+	c->mixed.sms = c->sms;
+	goto out;
+fail:
+	gray_destroy(c);
+	c = nullptr;
+out:
+	if(status)
+		*status = st;
+	return c;
+}
+
+static void
+free_grid(gray_ctx *c)
+{
+	if(!c->grid)
+		return;
+	Grid *g = c->grid;
+	size_t npts = (size_t)g->desc.nx * g->desc.ny * g->desc.nz;
+	for(int l = 0; l < 2; ++l)
+		dfree(c, g->lvl[l], npts * GRAY_NSTRIDE * sizeof(float));
+	const int n[3] = {g->desc.nx, g->desc.ny, g->desc.nz};
+	for(int a = 0; a < 3; ++a) {
+		dfree(c, g->nodes[a], (n[a] + 1) * sizeof(double));
+		dfree(c, g->nodes_f[a], (n[a] + 1) * sizeof(float));
+	}
+	delete g;
+	c->grid = nullptr;
+}
+
+extern "C" void
+gray_destroy(gray_ctx *c)
+{
+	if(!c)
+		return;
+	cudaSetDevice(c->device);
+	if(c->stream)
+		cudaStreamSynchronize(c->stream);
+	for(auto &kv : c->renders) {
+		Render *r = kv.second;
+		dfree(c, r->d_data, r->bytes);
+		delete r;
+	}
+	c->renders.clear();
+	free_grid(c);
+	if(c->ev0) cudaEventDestroy(c->ev0);
+	if(c->ev1) cudaEventDestroy(c->ev1);
+	if(c->own) cudaStreamDestroy(c->own);
+	delete c;
+}
+
+extern "C" int
+gray_set_stream(gray_ctx *c, void *stream)
+{
+	if(!c)
+		return GRAY_EINVAL;
+	c->stream = stream ? (cudaStream_t)stream : c->own;
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_sync(gray_ctx *c)
+{
+	if(!c)
+		return GRAY_EINVAL;
+	CK(cudaSetDevice(c->device));
+	CK(cudaStreamSynchronize(c->stream));
+	return GRAY_OK;
+}
+
+extern "C" size_t
+gray_hbm_used(const gray_ctx *c)
+{
+	return c ? c->used : 0;
+}
+
+/* One device block per render: data | info | steps | queue */
+extern "C" int
+gray_render_create(gray_ctx *c, const gray_render_desc *d, int *id)
+{
+	if(!c || !id)
+		return GRAY_EINVAL;
+	int st = check_desc(d);
+	if(st)
+		return st;
+	CK(cudaSetDevice(c->device));
+	Render *r = new(std::nothrow) Render;
+	if(!r)
+		return GRAY_ENOMEM;
+	r->desc = *d;
+	make_params(d, &r->p);
+	const size_t nr = (size_t)r->p.n_rays;
+	const size_t data_b = nr * r->p.n_data * sizeof(double);
+	const size_t info_b = nr * sizeof(double);
+	const size_t tab_b = (sizeof(MixedRender) + 255) / 256 * 256;
+	r->bytes = data_b + info_b + 256 + tab_b;
+	void *base = nullptr;
+	st = dalloc(c, &base, r->bytes);
+	if(st) {
+		delete r;
+		return st;
+	}
+	r->d_data  = (double *)base;
+	r->d_info  = (double *)((char *)base + data_b);
+	r->d_steps = (unsigned long long *)((char *)base + data_b + info_b);
+	r->d_queue = (unsigned int *)((char *)base + data_b + info_b + 128);
+	r->d_prefix = (unsigned long long *)((char *)base + data_b + info_b + 192);
+	r->d_table = (MixedRender *)((char *)base + data_b + info_b + 256);
+	CK(cudaMemsetAsync((char *)base + data_b + info_b, 0, 256, c->stream));
+	*id = c->next_id++;
+	c->renders[*id] = r;
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_render_destroy(gray_ctx *c, int id)
+{
+	Render *r = find(c, id);
+	if(!r)
+		return GRAY_ENOTFOUND;
+	CK(cudaSetDevice(c->device));
+	CK(cudaStreamSynchronize(c->stream));
+	dfree(c, r->d_data, r->bytes);
+	c->renders.erase(id);
+	delete r;
+	return GRAY_OK;
+}
+
+static int
+icond_impl(gray_ctx *c, Render *r)
+{
+	CK(cudaMemsetAsync(r->d_steps, 0, sizeof(unsigned long long), c->stream));
+	if(r->p.spacetime == GRAY_ST_NUMERICAL) {
+		if(!grid_ready(c))
+			return GRAY_ESTATE;
+		CK(launch_dyst_icond(r->p, c->grid->gp, r->d_data, r->d_info, c->stream));
+	} else {
+		CK(launch_icond64(r->p, r->d_data, r->d_info, c->stream));
+	}
+	r->has_state = true;
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_icond(gray_ctx *c, int id)
+{
+	Render *r = find(c, id);
+	if(!r)
+		return GRAY_ENOTFOUND;
+	CK(cudaSetDevice(c->device));
+	return icond_impl(c, r);
+}
+
+/* Build the one-entry render table of a mixed render and launch the
+ * persistent kernel over n_dump intervals starting at t_init. */
+static int
+run_mixed(gray_ctx *c, Render *r, double t_init, double dt_dump, long long n_dump,
+          long long n_sub)
+{
+	MixedRender m;
+	memset(&m, 0, sizeof(m));
+	fill_mixed_render(r->p, r->d_data, r->d_info, t_init, dt_dump, n_dump, n_sub, &m);
+	CK(cudaMemcpyAsync(r->d_table, &m, sizeof(m), cudaMemcpyHostToDevice, c->stream));
+	MixedTable T;
+	T.renders = r->d_table;
+	T.prefix = r->d_prefix; /* zeroed at creation: the one render starts at 0 */
+	T.n_renders = 1;
+	T.total = (unsigned long long)r->p.n_rays;
+	CK(launch_mixed_table(T, r->p.n_freq, r->d_queue, r->d_steps, c->stream, c->mixed));
+	return GRAY_OK;
+}
+
+static int
+evolve_interval(gray_ctx *c, Render *r, double t, double target, uint64_t n_sub)
+{
+	const double dt = target - t;
+	if(r->p.spacetime == GRAY_ST_NUMERICAL) {
+		if(!grid_ready(c))
+			return GRAY_ESTATE;
+		if(r->desc.precision == GRAY_PREC_FP64)
+			CK(launch_dyst_evolve64(r->p, c->grid->gp, r->d_data, r->d_info, dt,
+			                        (long long)n_sub, r->d_steps, c->stream));
+		else
+			CK(launch_dyst_mixed(r->p, c->grid->gp, r->d_data, r->d_info, t, dt, 1,
+			                     (long long)n_sub, r->d_steps, r->d_queue, c->stream,
+			                     c->mixed));
+		return GRAY_OK;
+	}
+	if(r->desc.precision == GRAY_PREC_FP64) {
+		CK(launch_evolve64(r->p, r->d_data, r->d_info, dt, (long long)n_sub,
+		                   r->d_steps, c->stream, c->evolve64_block));
+		return GRAY_OK;
+	}
+	return run_mixed(c, r, t, dt, 1, (long long)n_sub);
+}
+
+extern "C" int
+gray_evolve(gray_ctx *c, int id, double t, double target, uint64_t n_sub, double *ns)
+{
+	Render *r = find(c, id);
+	if(!r)
+		return GRAY_ENOTFOUND;
+	if(!r->has_state)
+		return GRAY_ESTATE;
+	if(n_sub == 0 || n_sub > (uint64_t)INT32_MAX || !std::isfinite(t) ||
+	   !std::isfinite(target))
+		return GRAY_EINVAL;
+	CK(cudaSetDevice(c->device));
+	int st = timed_begin(c);
+	if(st)
+		return st;
+	st = evolve_interval(c, r, t, target, n_sub);
+	if(st)
+		return st;
+	return timed_end(c, ns);
+}
+
+static int
+evolve_all_impl(gray_ctx *c, Render *r)
+{
+	const gray_render_desc &d = r->desc;
+	int st;
+	if(d.precision == GRAY_PREC_MIXED) {
+		if(r->p.spacetime == GRAY_ST_NUMERICAL)
+			CK(launch_dyst_mixed(r->p, c->grid->gp, r->d_data, r->d_info, d.t_init,
+			                     d.dt_dump, (long long)d.n_dump, (long long)d.n_sub,
+			                     r->d_steps, r->d_queue, c->stream, c->mixed));
+		else {
+			st = run_mixed(c, r, d.t_init, d.dt_dump, (long long)d.n_dump,
+			               (long long)d.n_sub);
+			if(st)
+				return st;
+		}
+	} else {
+		/* sim-org/gray.c:248-257 */
+		for(uint64_t i = 0; i < d.n_dump;) {
+			double t      = d.t_init + (double)i * d.dt_dump;
+			double target = d.t_init + (double)(++i) * d.dt_dump;
+			st = evolve_interval(c, r, t, target, d.n_sub);
+			if(st)
+				return st;
+		}
+	}
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_run(gray_ctx *c, int id, double *ns)
+{
+	Render *r = find(c, id);
+	if(!r)
+		return GRAY_ENOTFOUND;
+	CK(cudaSetDevice(c->device));
+	int st = timed_begin(c);
+	if(!st)
+		st = icond_impl(c, r);
+	if(!st)
+		st = evolve_all_impl(c, r);
+	if(!st)
+		st = timed_end(c, ns);
+	return st;
+}
+
+extern "C" int
+gray_evolve_all(gray_ctx *c, int id, double *ns)
+{
+	Render *r = find(c, id);
+	if(!r)
+		return GRAY_ENOTFOUND;
+	if(!r->has_state)
+		return GRAY_ESTATE;
+	CK(cudaSetDevice(c->device));
+	int st = timed_begin(c);
+	if(!st)
+		st = evolve_all_impl(c, r);
+	if(!st)
+		st = timed_end(c, ns);
+	return st;
+}
+
+extern "C" int
+gray_read_state(gray_ctx *c, int id, void *data, size_t data_bytes, void *info,
+                size_t info_bytes, int layout)
+{
+	Render *r = find(c, id);
+	if(!r)
+		return GRAY_ENOTFOUND;
+	if(!r->has_state)
+		return GRAY_ESTATE;
+	if(layout != GRAY_LAYOUT_SOA && layout != GRAY_LAYOUT_AOS)
+		return GRAY_EINVAL;
+	const size_t nr = (size_t)r->p.n_rays;
+	const size_t db = nr * r->p.n_data * sizeof(double);
+	if(data && data_bytes != db)
+		return GRAY_ESIZE;
+	if(info && info_bytes != nr * sizeof(double))
+		return GRAY_ESIZE;
+	CK(cudaSetDevice(c->device));
+	if(data) {
+		if(layout == GRAY_LAYOUT_SOA) {
+			CK(cudaMemcpyAsync(data, r->d_data, db, cudaMemcpyDeviceToHost, c->stream));
+		} else {
+			void *tmp = nullptr;
+			int st = dalloc(c, &tmp, db);
+			if(st)
+				return st;
+			cudaError_t e = launch_transpose(r->d_data, (double *)tmp, (long long)nr,
+			                                 r->p.n_data, 1, c->stream);
+			if(e == cudaSuccess)
+				e = cudaMemcpyAsync(data, tmp, db, cudaMemcpyDeviceToHost, c->stream);
+			if(e == cudaSuccess)
+				e = cudaStreamSynchronize(c->stream);
+			dfree(c, tmp, db);
+			if(e != cudaSuccess)
+				return from_cuda(e);
+		}
+	}
+	if(info)
+		CK(cudaMemcpyAsync(info, r->d_info, nr * sizeof(double), cudaMemcpyDeviceToHost,
+		                   c->stream));
+	CK(cudaStreamSynchronize(c->stream));
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_write_state(gray_ctx *c, int id, const void *data, size_t data_bytes, int layout)
+{
+	Render *r = find(c, id);
+	if(!r)
+		return GRAY_ENOTFOUND;
+	if(!data || (layout != GRAY_LAYOUT_SOA && layout != GRAY_LAYOUT_AOS))
+		return GRAY_EINVAL;
+	const size_t nr = (size_t)r->p.n_rays;
+	const size_t db = nr * r->p.n_data * sizeof(double);
+	if(data_bytes != db)
+		return GRAY_ESIZE;
+	CK(cudaSetDevice(c->device));
+	if(layout == GRAY_LAYOUT_SOA) {
+		CK(cudaMemcpyAsync(r->d_data, data, db, cudaMemcpyHostToDevice, c->stream));
+	} else {
+		void *tmp = nullptr;
+		int st = dalloc(c, &tmp, db);
+		if(st)
+			return st;
+		cudaError_t e = cudaMemcpyAsync(tmp, data, db, cudaMemcpyHostToDevice, c->stream);
+		if(e == cudaSuccess)
+			e = launch_transpose((const double *)tmp, r->d_data, (long long)nr,
+			                     r->p.n_data, 0, c->stream);
+		if(e == cudaSuccess)
+			e = cudaStreamSynchronize(c->stream);
+		dfree(c, tmp, db);
+		if(e != cudaSuccess)
+			return from_cuda(e);
+	}
+	if(r->p.spacetime == GRAY_ST_KERR)
+		CK(launch_getuu64(r->p, r->d_data, r->d_info, c->stream));
+	CK(cudaMemsetAsync(r->d_steps, 0, sizeof(unsigned long long), c->stream));
+	CK(cudaStreamSynchronize(c->stream));
+	r->has_state = true;
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_read_kdown(gray_ctx *c, int id, double *k, size_t bytes)
+{
+	Render *r = find(c, id);
+	if(!r)
+		return GRAY_ENOTFOUND;
+	if(!r->has_state)
+		return GRAY_ESTATE;
+	if(!k)
+		return GRAY_EINVAL;
+	if(r->p.spacetime != GRAY_ST_KERR)
+		return GRAY_EINVAL;
+	const size_t nr = (size_t)r->p.n_rays;
+	if(bytes != nr * 4 * sizeof(double))
+		return GRAY_ESIZE;
+	CK(cudaSetDevice(c->device));
+	void *tmp = nullptr;
+	int st = dalloc(c, &tmp, bytes);
+	if(st)
+		return st;
+	cudaError_t e = launch_kdown64(r->p, r->d_data, (double *)tmp, c->stream);
+	if(e == cudaSuccess)
+		e = cudaMemcpyAsync(k, tmp, bytes, cudaMemcpyDeviceToHost, c->stream);
+	if(e == cudaSuccess)
+		e = cudaStreamSynchronize(c->stream);
+	dfree(c, tmp, bytes);
+	return from_cuda(e);
+}
+
+extern "C" int
+gray_ray_steps(gray_ctx *c, int id, uint64_t *steps)
+{
+	Render *r = find(c, id);
+	if(!r)
+		return GRAY_ENOTFOUND;
+	if(!steps)
+		return GRAY_EINVAL;
+	CK(cudaSetDevice(c->device));
+	unsigned long long v = 0;
+	CK(cudaMemcpyAsync(&v, r->d_steps, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
+	CK(cudaStreamSynchronize(c->stream));
+	*steps = v;
+	return GRAY_OK;
+}
+
+/* ---- numerical spacetime ------------------------------------------- */
+
+static int
+check_grid(const gray_grid_desc *g)
+{
+	if(!g || g->nx < 2 || g->ny < 2 || g->nz < 2)
+		return GRAY_EINVAL;
+	if((long long)g->nx * g->ny * g->nz > (1ll << 28))
+		return GRAY_EINVAL;
+	for(int a = 1; a <= 3; ++a)
+		if(!(g->box[a] < g->box[a + 4]))
+			return GRAY_EINVAL;
+	if(!(g->box[4] >= g->box[0]))
+		return GRAY_EINVAL;
+	return GRAY_OK;
+}
+
+static int
+same_shape(const gray_grid_desc *a, const gray_grid_desc *b)
+{
+	return a->nx == b->nx && a->ny == b->ny && a->nz == b->nz &&
+	       memcmp(a->box + 1, b->box + 1, 3 * sizeof(float)) == 0 &&
+	       memcmp(a->box + 5, b->box + 5, 3 * sizeof(float)) == 0;
+}
+
+/* (Re)creates the grid when the shape changes; computes the fisheye
+ * constants and node tables of interp.cl:89-121 on the host in FP64. */
+static int
+ensure_grid(gray_ctx *c, const gray_grid_desc *gd)
+{
+	if(c->grid && !same_shape(&c->grid->desc, gd))
+		free_grid(c);
+	if(!c->grid) {
+		Grid *g = new(std::nothrow) Grid;
+		if(!g)
+			return GRAY_ENOMEM;
+		g->desc = *gd;
+		c->grid = g;
+		size_t npts = (size_t)gd->nx * gd->ny * gd->nz;
+		for(int l = 0; l < 2; ++l) {
+			int st = dalloc(c, (void **)&g->lvl[l], npts * GRAY_NSTRIDE * sizeof(float));
+			if(st) {
+				free_grid(c);
+				return st;
+			}
+		}
+		const int n[3] = {gd->nx, gd->ny, gd->nz};
+		GridParams &gp = g->gp;
+		memset(&gp, 0, sizeof(gp));
+		for(int a = 0; a < 3; ++a) {
+			double lo = gd->box[a + 1], hi = gd->box[a + 5];
+			double B = cbrt(asinh(lo));
+			double A = (cbrt(asinh(hi)) - B) / (double)(n[a] - 1);
+			gp.A[a] = A;
+			gp.B[a] = B;
+			std::vector<double> nd(n[a] + 1);
+			std::vector<float> nf(n[a] + 1);
+			for(int i = 0; i <= n[a]; ++i) {
+				double f = fma(A, (double)i, B);
+				nd[i] = sinh((f * f) * f);
+				nf[i] = (float)nd[i];
+			}
+			int st = dalloc(c, (void **)&g->nodes[a], (n[a] + 1) * sizeof(double));
+			if(!st)
+				st = dalloc(c, (void **)&g->nodes_f[a], (n[a] + 1) * sizeof(float));
+			if(st) {
+				free_grid(c);
+				return st;
+			}
+			CK(cudaMemcpy(g->nodes[a], nd.data(), (n[a] + 1) * sizeof(double),
+			              cudaMemcpyHostToDevice));
+			CK(cudaMemcpy(g->nodes_f[a], nf.data(), (n[a] + 1) * sizeof(float),
+			              cudaMemcpyHostToDevice));
+			gp.nodes[a] = g->nodes[a];
+			gp.nodes_f[a] = g->nodes_f[a];
+		}
+		gp.nx = gd->nx; gp.ny = gd->ny; gp.nz = gd->nz;
+		gp.lvl[0] = g->lvl[0];
+		gp.lvl[1] = g->lvl[1];
+	}
+	Grid *g = c->grid;
+	g->desc.box[0] = gd->box[0];
+	g->desc.box[4] = gd->box[4];
+	g->desc.bug_gzz = gd->bug_gzz;
+	g->desc.physics = gd->physics;
+	memcpy(g->gp.box, g->desc.box, sizeof(g->gp.box));
+	g->gp.bug_gzz = gd->bug_gzz;
+	g->gp.physics = gd->physics;
+	g->gp.single = gd->box[0] == gd->box[4];
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_load_spacetime_interleaved(gray_ctx *c, const gray_grid_desc *gd,
+                                const float *fields, int level)
+{
+	if(!c || !fields || (level != 0 && level != 1))
+		return GRAY_EINVAL;
+	int st = check_grid(gd);
+	if(st)
+		return st;
+	CK(cudaSetDevice(c->device));
+	st = ensure_grid(c, gd);
+	if(st)
+		return st;
+	const size_t npts = (size_t)gd->nx * gd->ny * gd->nz;
+	/* host rows of 51 -> device rows of GRAY_NSTRIDE (pitched copy) */
+	CK(cudaMemcpy2DAsync(c->grid->lvl[level], GRAY_NSTRIDE * sizeof(float), fields,
+	                     GRAY_NCOMP * sizeof(float), GRAY_NCOMP * sizeof(float), npts,
+	                     cudaMemcpyHostToDevice, c->stream));
+	CK(cudaStreamSynchronize(c->stream));
+	c->grid->loaded[level] = true;
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_load_spacetime(gray_ctx *c, const gray_grid_desc *gd, const float *const *fields,
+                    int level)
+{
+	if(!c || !fields || (level != 0 && level != 1))
+		return GRAY_EINVAL;
+	for(int i = 0; i < GRAY_NCOMP; ++i)
+		if(!fields[i])
+			return GRAY_EINVAL;
+	int st = check_grid(gd);
+	if(st)
+		return st;
+	CK(cudaSetDevice(c->device));
+	st = ensure_grid(c, gd);
+	if(st)
+		return st;
+	const size_t npts = (size_t)gd->nx * gd->ny * gd->nz;
+	/* stage one field at a time and scatter it into the interleaved rows */
+	CK(cudaMemcpy2DAsync(c->grid->lvl[level], GRAY_NSTRIDE * sizeof(float), fields[0],
+	                     sizeof(float), sizeof(float), npts, cudaMemcpyHostToDevice,
+	                     c->stream));
+	for(int i = 1; i < GRAY_NCOMP; ++i)
+		CK(cudaMemcpy2DAsync(c->grid->lvl[level] + i, GRAY_NSTRIDE * sizeof(float),
+		                     fields[i], sizeof(float), sizeof(float), npts,
+		                     cudaMemcpyHostToDevice, c->stream));
+	CK(cudaStreamSynchronize(c->stream));
+	c->grid->loaded[level] = true;
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_make_boosted_ks(gray_ctx *c, const gray_grid_desc *gd, double a, double v,
+                     int axis, double t, int level)
+{
+	if(!c || (level != 0 && level != 1) || axis < 1 || axis > 3)
+		return GRAY_EINVAL;
+	if(!(a > -1.0 && a < 1.0) || !(v > -1.0 && v < 1.0))
+		return GRAY_EINVAL;
+	int st = check_grid(gd);
+	if(st)
+		return st;
+	CK(cudaSetDevice(c->device));
+	st = ensure_grid(c, gd);
+	if(st)
+		return st;
+	CK(launch_boosted_ks(c->grid->gp, c->grid->lvl[level], a, v, axis, t, c->stream));
+	CK(cudaStreamSynchronize(c->stream));
+	c->grid->loaded[level] = true;
+	return GRAY_OK;
+}
+
+cudaError_t measure_peak(int precision, int sms, cudaStream_t st, double *flops);
+
+extern "C" int
+gray_measure_peak(gray_ctx *c, int precision, double *flops)
+{
+	if(!c || !flops || (precision != GRAY_PREC_FP64 && precision != GRAY_PREC_MIXED))
+		return GRAY_EINVAL;
+	CK(cudaSetDevice(c->device));
+	CK(measure_peak(precision, c->sms, c->stream, flops));
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_swap_levels(gray_ctx *c)
+{
+	if(!c || !c->grid)
+		return GRAY_ESTATE;
+	Grid *g = c->grid;
+	float *t = g->lvl[0];
+	g->lvl[0] = g->lvl[1];
+	g->lvl[1] = t;
+	bool b = g->loaded[0];
+	g->loaded[0] = g->loaded[1];
+	g->loaded[1] = b;
+	g->gp.lvl[0] = g->lvl[0];
+	g->gp.lvl[1] = g->lvl[1];
+	return GRAY_OK;
+}

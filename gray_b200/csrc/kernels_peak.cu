@@ -1,0 +1,118 @@
+/*
+ * CUDA-core peak microbenchmark: independent FMA chains per thread, enough
+ * warps to fill every SM.  Gives the FP32 and FP64 denominators of the
+ * roofline of the geodesic kernels (which are CUDA-core bound, not
+ * tensor-core or HBM bound).  FP32 is measured both with scalar FFMA and
+ * with the packed f32x2 FMA of sm_100; the larger rate is reported.
+ */
+#include "gray_internal.h"
+
+namespace {
+
+constexpr int CHAINS = 8;
+
+__global__ void __launch_bounds__(256)
+fma32_kernel(float *out, int iters, float a, float b)
+{
+	float v[CHAINS];
+#pragma unroll
+	for(int c = 0; c < CHAINS; ++c)
+		v[c] = threadIdx.x * 1e-3f + c;
+	for(int i = 0; i < iters; ++i) {
+#pragma unroll
+		for(int c = 0; c < CHAINS; ++c)
+			v[c] = fmaf(v[c], a, b);
+	}
+	float s = 0.0f;
+#pragma unroll
+	for(int c = 0; c < CHAINS; ++c)
+		s += v[c];
+	if(s == 12345.678f)
+		out[0] = s; /* keeps the chains alive */
+}
+
+__global__ void __launch_bounds__(256)
+fma32x2_kernel(float *out, int iters, float a, float b)
+{
+	float2 v[CHAINS];
+	const float2 A = make_float2(a, a), B = make_float2(b, b);
+#pragma unroll
+	for(int c = 0; c < CHAINS; ++c)
+		v[c] = make_float2(threadIdx.x * 1e-3f + c, c + 0.5f);
+	for(int i = 0; i < iters; ++i) {
+#pragma unroll
+		for(int c = 0; c < CHAINS; ++c)
+			v[c] = __ffma2_rn(v[c], A, B);
+	}
+	float s = 0.0f;
+#pragma unroll
+	for(int c = 0; c < CHAINS; ++c)
+		s += v[c].x + v[c].y;
+	if(s == 12345.678f)
+		out[0] = s;
+}
+
+__global__ void __launch_bounds__(256)
+fma64_kernel(double *out, int iters, double a, double b)
+{
+	double v[CHAINS];
+#pragma unroll
+	for(int c = 0; c < CHAINS; ++c)
+		v[c] = threadIdx.x * 1e-3 + c;
+	for(int i = 0; i < iters; ++i) {
+#pragma unroll
+		for(int c = 0; c < CHAINS; ++c)
+			v[c] = fma(v[c], a, b);
+	}
+	double s = 0.0;
+#pragma unroll
+	for(int c = 0; c < CHAINS; ++c)
+		s += v[c];
+	if(s == 12345.678)
+		out[0] = s;
+}
+
+} /* namespace */
+
+/* Returns FLOP/s (FMA = 2 FLOP) of the best of `reps` timed launches. */
+cudaError_t
+measure_peak(int precision, int sms, cudaStream_t st, double *flops)
+{
+	const int block = 256, iters = 1 << 14, reps = 5;
+	const unsigned grid = (unsigned)sms * 8;
+	void *buf = nullptr;
+	cudaEvent_t e0, e1;
+	cudaError_t e = cudaMalloc(&buf, 64);
+	if(e != cudaSuccess)
+		return e;
+	cudaEventCreate(&e0);
+	cudaEventCreate(&e1);
+	double best = 0.0;
+	const double threads = (double)grid * block;
+	const int variants = precision == GRAY_PREC_FP64 ? 1 : 2;
+	for(int var = 0; var < variants && e == cudaSuccess; ++var) {
+		for(int r = 0; r < reps + 1 && e == cudaSuccess; ++r) {
+			cudaEventRecord(e0, st);
+			if(precision == GRAY_PREC_FP64)
+				fma64_kernel<<<grid, block, 0, st>>>((double *)buf, iters, 0.999999, 1e-7);
+			else if(var == 0)
+				fma32_kernel<<<grid, block, 0, st>>>((float *)buf, iters, 0.999999f, 1e-7f);
+			else
+				fma32x2_kernel<<<grid, block, 0, st>>>((float *)buf, iters, 0.999999f, 1e-7f);
+			cudaEventRecord(e1, st);
+			e = cudaEventSynchronize(e1);
+			if(e != cudaSuccess)
+				break;
+			float ms = 0.0f;
+			cudaEventElapsedTime(&ms, e0, e1);
+			double fl = threads * iters * CHAINS * 2.0 * (var == 1 ? 2.0 : 1.0);
+			if(r > 0 && ms > 0.0f && fl / (ms * 1e-3) > best)
+				best = fl / (ms * 1e-3);
+		}
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	cudaFree(buf);
+	*flops = best;
+	return e;
+}

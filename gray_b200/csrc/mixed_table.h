@@ -1,0 +1,42 @@
+/*
+ * Render table of the mixed-precision persistent kernels.  One entry per
+ * render: FP32 constants for the bulk arithmetic, FP64 copies for the FP64
+ * islands, the render's state buffers and its dump schedule.  A batch of
+ * renders (many cameras, spins, resolutions) is one table and one launch.
+ */
+#ifndef GRAY_MIXED_TABLE_H
+#define GRAY_MIXED_TABLE_H
+
+#include "gray_internal.h"
+
+struct MixedRender {
+	float  a, aa, rp, risco, eps_stop;
+	float  cdt_scale;          /* 0.01: the step fraction of phys.cl:60-61     */
+	float  kappa, n0_rp15, ihr2_log2e;
+	float  nupow[GRAY_MAX_FREQ];
+	float  nuinv2[GRAY_MAX_FREQ];
+	int    flow;
+	int    n_dump;
+	double a_d, aa_d, rp_d;    /* FP64 islands                                */
+	double *data, *info;       /* SoA FP64 state and getuu diagnostic         */
+	long long n_rays;
+	double t_init, dt_dump;
+	long long n_sub;
+};
+
+struct MixedTable {
+	const MixedRender *renders;        /* device array [n_renders]           */
+	const unsigned long long *prefix;  /* device array: first global index   */
+	int n_renders;
+	unsigned long long total;          /* rays over all renders              */
+};
+
+void fill_mixed_render(const RenderParams &p, double *data, double *info,
+                       double t_init, double dt_dump, long long n_dump,
+                       long long n_sub, MixedRender *m);
+
+cudaError_t launch_mixed_table(const MixedTable &T, int n_freq, unsigned int *queue,
+                               unsigned long long *steps, cudaStream_t st,
+                               const MixedLaunch &cfg);
+
+#endif /* GRAY_MIXED_TABLE_H */

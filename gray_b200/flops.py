@@ -1,0 +1,46 @@
+"""Algorithmic work per accepted RK4 ray-step, counted from the kernel source.
+
+Counting rule: an FMA is 2 FLOP; every add, multiply, divide, square root,
+reciprocal, reciprocal square root, exp/exp2/log2/pow is 1 FLOP; negation
+and copies are free.  Counts assume the ray is inside the emission region
+(r > r_isco, timelike Keplerian flow, shift > 0), which holds for nearly
+every step of the torus workloads; outside it the transfer part is skipped.
+
+Mixed kernel (gray_b200/csrc/kernels_mixed.cu), per call:
+  ks_rhs32        197  (head 42: radius root, f and its gradient with
+                        2 rsqrt + 2 rcp; l and its gradient 33; D tensors,
+                        contractions and the acceleration 122)
+  torus_rt32      46 + 6 per frequency  (Keplerian flow 34, density 8 with
+                        1 ex2, shift^-0.7 with lg2 + ex2, 1 ex2 per frequency)
+  RK4 + Kahan     per component: stages 2 + 4 + 4, final 2 + 4 (Kahan)
+                  = 16, plus 3 scalars
+  step control    17  (FP32 radius root and the n/|dt| tick rule)
+
+FP64 kernel (gray_b200/csrc/kernels_fp64.cu), per call:
+  ks_rhs64        196  (5 divides and 2 sqrt counted as 1 each)
+  torus_rt64      49 + 5 per frequency  (pow and exp counted as 1 each)
+  RK4             per component 2 + 2 + 2 + 6 = 12, plus 2 scalars
+  step control    16 + 4 for the integer-tick arithmetic
+
+The reference's own comments count the same KS RHS as about 205 FLOP
+(KS.cl:310-374), counting its divides the same way.
+"""
+
+
+def mixed_per_step(n_freq, transfer=True):
+    nd = 8 + 2 * n_freq
+    rhs = 197 + ((46 + 6 * n_freq) if (transfer and n_freq) else 0)
+    return 4 * rhs + 16 * nd + 3 + 17
+
+
+def fp64_per_step(n_freq, transfer=True):
+    nd = 8 + 2 * n_freq
+    rhs = 196 + ((49 + 5 * n_freq) if (transfer and n_freq) else 0)
+    return 4 * rhs + 12 * nd + 2 + 20
+
+
+def state_bytes_per_ray(n_freq):
+    """HBM traffic of one persistent launch per ray: FP64 initial state in,
+    FP64 final state and the getuu diagnostic out."""
+    nd = 8 + 2 * n_freq
+    return 8 * nd + 8 * nd + 8

@@ -1,0 +1,206 @@
+/*
+ * libgray_cuda -- B200 (sm_100a) geodesic hot path of GRay2 behind a C ABI.
+ *
+ * The reference (luxsrc/gray) reaches its OpenCL kernels through the lux
+ * opencl module: sim-org/build.c:30-143 JIT-builds the program,
+ * sim-org/icond.c:29-86 launches icond_drv, sim-org/evolve.c:28-67 launches
+ * evolve_drv once per dump interval and returns the kernel time in ns, and
+ * sim-org/io.c:39-72 maps the ray buffers back to the host.  In the new lux
+ * tree (sim/gray.c:116-176) the same steps are dmk() of real[8] rays,
+ * ic->init(), the planner's exec (a TODO at sim/gray.c:168) and ocl->d2h().
+ * This header replaces that glue with plain C entry points: no CUDA or
+ * torch types cross it; the context owns every device allocation, and hosts
+ * pass host pointers with explicit byte counts.
+ *
+ * Errors: every entry point returns an int status (0 = GRAY_OK, negative =
+ * GRAY_E*), never aborts; gray_strerror() names it.  Threading: one context
+ * per host thread, except gray_serve_submit / gray_serve_poll, which lock.
+ */
+#ifndef GRAY_CUDA_H
+#define GRAY_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GRAY_ABI_VERSION 1
+#define GRAY_MAX_FREQ    8
+
+enum gray_status {
+	GRAY_OK        =  0,
+	GRAY_EINVAL    = -1,  /* bad argument or configuration        */
+	GRAY_ENOMEM    = -2,  /* device or host allocation failed      */
+	GRAY_ECUDA     = -3,  /* CUDA runtime error                    */
+	GRAY_ENODEV    = -4,  /* no usable sm_100 device               */
+	GRAY_EBUDGET   = -5,  /* request exceeds the HBM budget        */
+	GRAY_ETIMEOUT  = -6,  /* bounded device wait ran out           */
+	GRAY_ENOTFOUND = -7,  /* unknown render / request id           */
+	GRAY_ESTATE    = -8,  /* call out of order (e.g. no icond yet) */
+	GRAY_ESIZE     = -9   /* host buffer size does not match       */
+};
+
+enum gray_precision {
+	GRAY_PREC_FP64  = 0,  /* plain FP64 (sim-org/setup.opts:11 precision=8) */
+	GRAY_PREC_MIXED = 1   /* FP32 bulk, FP64 islands, compensated update    */
+};
+
+enum gray_spacetime {
+	GRAY_ST_KERR      = 0, /* analytic Cartesian Kerr-Schild (KS.cl)         */
+	GRAY_ST_NUMERICAL = 1  /* interpolated grid (dyst.cl + interp.cl)        */
+};
+
+enum gray_flow {
+	GRAY_FLOW_NONE  = 0,   /* geodesics only (n_freq ignored)               */
+	GRAY_FLOW_TORUS = 1    /* analytic power-law torus feeding rt.cl form   */
+};
+
+enum gray_term {
+	GRAY_TERM_EPS   = 0,   /* reference: stop when r - r_+ < 0.01 (phys.cl:54) */
+	GRAY_TERM_RPLUS = 1    /* stop when r < 1.01 r_+                          */
+};
+
+enum gray_layout {
+	GRAY_LAYOUT_SOA = 0,   /* data[s * n_rays + g]  (sim-org/SoA.cl:29)      */
+	GRAY_LAYOUT_AOS = 1    /* data[g * n_data + s]  (sim-org/AoS.cl:29)      */
+};
+
+/* One render: the run-time parameters of sim/gray.opts, sim/Kerr.opts,
+ * sim/infcam.opts, sim-org/setup.opts and sim-org/param.opts that the hot
+ * path reads, with the reference's names. */
+typedef struct gray_render_desc {
+	/* Kerr.opts */
+	double   m_bh;            /* m_bh:M   solar masses (transfer units only) */
+	double   a_spin;          /* a_spin:a dimensionless spin                  */
+	/* infcam.opts */
+	double   w_img, h_img;    /* w_img:w, h_img:h   image size in GM/c^2      */
+	double   r_obs;           /* r_obs:r  camera distance                     */
+	double   i_obs, j_obs;    /* i_obs:i, j_obs:j   degrees                   */
+	uint64_t n_width;         /* n_width:W  rays along the width             */
+	uint64_t n_height;        /* n_height:H rays along the height            */
+	/* gray.opts / setup.opts step control and output times */
+	double   t_init;          /* t_init:t0                                    */
+	double   dt_dump;         /* dt_dump:dt  affine interval between dumps    */
+	uint64_t n_sub;           /* n_sub:n  substeps per dump (step-size cap)   */
+	uint64_t n_dump;          /* n_dump:N number of dump intervals            */
+	int32_t  term;            /* enum gray_term                               */
+	/* radiative transfer (param.opts nu list) */
+	int32_t  n_freq;          /* 0 .. GRAY_MAX_FREQ                            */
+	double   nu[GRAY_MAX_FREQ];
+	int32_t  flow;            /* enum gray_flow                               */
+	double   torus_n0;        /* density normalisation                        */
+	double   torus_kappa;     /* absorption normalisation                     */
+	double   torus_hr;        /* scale height over radius                     */
+	/* selection */
+	int32_t  spacetime;       /* enum gray_spacetime                          */
+	int32_t  precision;       /* enum gray_precision                          */
+} gray_render_desc;
+
+typedef struct gray_ctx gray_ctx;
+
+/* ---- context ------------------------------------------------------- */
+
+const char *gray_strerror(int status);
+int         gray_abi_version(void);
+
+/* Replaces lux_load("opencl", &opts) (sim/gray.c:88-95; sim-org/build.c:134-142):
+ * binds CUDA device `device` (the i_device:id option) and caps the HBM the
+ * context may allocate at hbm_budget bytes (0 = 90% of free memory). */
+gray_ctx   *gray_create(int device, size_t hbm_budget, int *status);
+void        gray_destroy(gray_ctx *ctx);
+
+/* Launch on a caller-provided cudaStream_t (passed as void *); NULL returns
+ * to the context's own stream. */
+int         gray_set_stream(gray_ctx *ctx, void *cuda_stream);
+int         gray_sync(gray_ctx *ctx);
+size_t      gray_hbm_used(const gray_ctx *ctx);
+
+/* ---- renders ------------------------------------------------------- */
+
+/* Replaces the buffer set-up of sim-org/gray.c:113-145 (_init: data and
+ * info buffers of n_rays * n_data reals) and sim/gray.c:115-117 (dmk of
+ * real[8] rays).  State is kept on the device in SoA order. */
+int gray_render_create(gray_ctx *ctx, const gray_render_desc *desc, int *render_id);
+int gray_render_destroy(gray_ctx *ctx, int render_id);
+
+/* Replaces icond() (sim-org/icond.c:29-86 -> driver.cl:36-67 icond_drv) and
+ * the infcam initcond plug-in's init (sim/gray/infcam.c:37-42). */
+int gray_icond(gray_ctx *ctx, int render_id);
+
+/* Replaces evolve() (sim-org/evolve.c:28-67 -> driver.cl:69-108 evolve_drv):
+ * integrates every ray over one dump interval of affine length target - t
+ * with n_sub substeps.  If ns is non-NULL the call waits and stores the
+ * kernel time in ns (what ocl->exec returns); otherwise it only enqueues. */
+int gray_evolve(gray_ctx *ctx, int render_id, double t, double target,
+                uint64_t n_sub, double *ns);
+
+/* icond + all n_dump intervals of the render (the sim-org/gray.c:243-294
+ * loop without the intermediate dumps).  FP64 renders run the per-interval
+ * kernel like the reference; mixed renders run one persistent launch. */
+int gray_run(gray_ctx *ctx, int render_id, double *ns);
+
+/* The evolve part of gray_run alone: all n_dump intervals from the current
+ * state (after gray_icond or gray_write_state). */
+int gray_evolve_all(gray_ctx *ctx, int render_id, double *ns);
+
+/* Replaces dump()'s ocl->mmap (sim-org/io.c:39-72) and sim/gray.c:170-172
+ * d2h: copies the FP64 state (n_rays * n_data doubles) and the getuu()
+ * diagnostic (n_rays doubles) to host memory in the requested layout.
+ * Either pointer may be NULL. */
+int gray_read_state(gray_ctx *ctx, int render_id, void *data, size_t data_bytes,
+                    void *info, size_t info_bytes, int layout);
+
+/* Upload a state (resume from a dump; io.c:37 leaves load() as a TODO). */
+int gray_write_state(gray_ctx *ctx, int render_id, const void *data,
+                     size_t data_bytes, int layout);
+
+/* Covariant momentum k_mu = g_mu_nu u^nu per ray (KS.cl:91-114 down()),
+ * n_rays * 4 doubles in SoA order. */
+int gray_read_kdown(gray_ctx *ctx, int render_id, double *k, size_t bytes);
+
+/* Accepted RK4 steps summed over the render's rays since the last icond. */
+int gray_ray_steps(gray_ctx *ctx, int render_id, uint64_t *steps);
+
+/* ---- numerical spacetime (sim-org/io.c:302-533, interp.cl, dyst.cl) - */
+
+typedef struct gray_grid_desc {
+	int32_t nx, ny, nz;  /* points along x, y, z (num_points.s123)         */
+	float   box[8];      /* {t1, xmin, ymin, zmin, t2, xmax, ymax, zmax}     */
+	int32_t bug_gzz;     /* 1: read g_zz from g_yz as dyst.cl:283 does      */
+	int32_t physics;     /* 1: flat outside the box, time factor in [0,1]   */
+} gray_grid_desc;
+
+/* Upload one time level (0 = t1, 1 = t2) of 51 FP32 fields, each nz*ny*nx
+ * in [z][y][x] order, in the order of io.c:356-428: Gamma_ijk (i-major,
+ * j <= k; 40), g_ij (i <= j; 10), rho.  fields[51] are host pointers. */
+int gray_load_spacetime(gray_ctx *ctx, const gray_grid_desc *grid,
+                        const float *const *fields, int level);
+
+/* Same, but the fields are already interleaved [z][y][x][51] in one host
+ * array of nz*ny*nx*51 floats. */
+int gray_load_spacetime_interleaved(gray_ctx *ctx, const gray_grid_desc *grid,
+                                    const float *fields, int level);
+
+/* Sample boosted Kerr-Schild (mass 1, spin a, speed v along axis 1..3) on
+ * the device at time t into level `level` of the context's grid: the
+ * generator of tools/generate_data.py + tools/boosted_ks.py run as a kernel. */
+int gray_make_boosted_ks(gray_ctx *ctx, const gray_grid_desc *grid, double a,
+                         double v, int axis, double t, int level);
+
+/* Swap the two time levels (io.c:279-300 copy_snapshot). */
+int gray_swap_levels(gray_ctx *ctx);
+
+/* ---- measurement (no reference counterpart) ------------------------ */
+
+/* CUDA-core FMA-loop peak of the context's device in FLOP/s (FMA = 2):
+ * the roofline denominator of the geodesic kernels.  precision selects
+ * FP64 or FP32 (best of scalar and packed f32x2 FMA). */
+int gray_measure_peak(gray_ctx *ctx, int precision, double *flops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRAY_CUDA_H */

@@ -1,0 +1,303 @@
+"""ctypes front end of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module, and only to check or time against the CUDA path.  The product
+package (gray_b200) never imports it.
+
+The C library (oracle/gray_oracle.c) is a plain FP64 restatement of the
+reference's OpenCL kernels (luxsrc/gray sim-org/KS.cl, phys.cl, RK4.cl,
+driver.cl, rt.cl, interp.cl, dyst.cl); see the citations there.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liborc.so")
+MAX_FREQ = 8
+TERM_EPS, TERM_RPLUS = 0, 1
+FLOW_NONE, FLOW_TORUS = 0, 1
+
+
+class OrcDesc(ctypes.Structure):
+    _fields_ = [
+        ("a_spin", ctypes.c_double),
+        ("w_img", ctypes.c_double), ("h_img", ctypes.c_double),
+        ("r_obs", ctypes.c_double), ("i_obs", ctypes.c_double),
+        ("j_obs", ctypes.c_double),
+        ("w_rays", ctypes.c_int64), ("h_rays", ctypes.c_int64),
+        ("t_init", ctypes.c_double), ("dt_dump", ctypes.c_double),
+        ("n_sub", ctypes.c_int64), ("n_dump", ctypes.c_int64),
+        ("term", ctypes.c_int),
+        ("n_freq", ctypes.c_int),
+        ("nu", ctypes.c_double * MAX_FREQ),
+        ("flow", ctypes.c_int),
+        ("torus_n0", ctypes.c_double), ("torus_kappa", ctypes.c_double),
+        ("torus_hr", ctypes.c_double),
+    ]
+
+
+class OrcGrid(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("box", ctypes.c_float * 8),
+        ("fields", ctypes.c_void_p * 2),
+        ("bug_gzz", ctypes.c_int),
+        ("physics", ctypes.c_int),
+    ]
+
+
+def build():
+    """Compile the oracle with its Makefile (plain gcc, no GPU needed)."""
+    subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER
+        d, i64 = ctypes.c_double, ctypes.c_int64
+        pd, pi64 = P(d), P(i64)
+        L.orc_getrr.restype = d
+        L.orc_getrr.argtypes = [d, pd]
+        L.orc_geteps.restype = d
+        L.orc_geteps.argtypes = [d, pd]
+        L.orc_down.argtypes = [d, pd, pd, pd]
+        L.orc_getuu.restype = d
+        L.orc_getuu.argtypes = [d, pd]
+        L.orc_ks_rhs.argtypes = [d, pd, pd]
+        L.orc_camera.argtypes = [P(OrcDesc), pd]
+        L.orc_icond.argtypes = [P(OrcDesc), pd, i64, pd]
+        L.orc_getdt.restype = d
+        L.orc_getdt.argtypes = [P(OrcDesc), pd, d]
+        L.orc_rhs.argtypes = [P(OrcDesc), pd, pd]
+        L.orc_integrate.argtypes = [P(OrcDesc), pd, d]
+        L.orc_evolve_ray.restype = i64
+        L.orc_evolve_ray.argtypes = [P(OrcDesc), pd, d, i64]
+        L.orc_trace.restype = ctypes.c_int
+        L.orc_trace.argtypes = [P(OrcDesc), pi64, i64, pd, pd, pi64, ctypes.c_int]
+        L.orc_evolve_states.restype = ctypes.c_int
+        L.orc_evolve_states.argtypes = [P(OrcDesc), pd, i64, pd, pi64, ctypes.c_int]
+        L.orc_rplus.restype = d
+        L.orc_rplus.argtypes = [d]
+        L.orc_risco.restype = d
+        L.orc_risco.argtypes = [d]
+        L.orc_interp.restype = d
+        L.orc_interp.argtypes = [P(OrcGrid), pd, ctypes.c_int]
+        L.orc_dyst_rhs.argtypes = [P(OrcGrid), pd, pd]
+        L.orc_dyst_down.argtypes = [P(OrcGrid), pd, pd, pd]
+        L.orc_dyst_icond.argtypes = [P(OrcDesc), pd, i64, pd]
+        L.orc_dyst_getdt.restype = d
+        L.orc_dyst_getdt.argtypes = [d]
+        L.orc_dyst_evolve_ray.restype = i64
+        L.orc_dyst_evolve_ray.argtypes = [P(OrcDesc), P(OrcGrid), pd, d, i64]
+        L.orc_dyst_trace.restype = ctypes.c_int
+        L.orc_dyst_trace.argtypes = [P(OrcDesc), P(OrcGrid), pi64, i64, pd, pd,
+                                     pi64, ctypes.c_int]
+        L.orc_boosted_ks.argtypes = [d, d, d, ctypes.c_int, pd, pd]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _pi(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+
+
+def make_desc(cfg):
+    """Build an OrcDesc from a plain dict using the .opts field names."""
+    d = OrcDesc()
+    d.a_spin = cfg.get("a_spin", 0.0)
+    d.w_img = cfg.get("w_img", 64.0)
+    d.h_img = cfg.get("h_img", 64.0)
+    d.r_obs = cfg.get("r_obs", 1024.0)
+    d.i_obs = cfg.get("i_obs", 60.0)
+    d.j_obs = cfg.get("j_obs", 0.0)
+    d.w_rays = cfg.get("n_width", 512)
+    d.h_rays = cfg.get("n_height", 512)
+    d.t_init = cfg.get("t_init", 0.0)
+    d.dt_dump = cfg.get("dt_dump", -32.0)
+    d.n_sub = cfg.get("n_sub", 1024)
+    d.n_dump = cfg.get("n_dump", 64)
+    d.term = cfg.get("term", TERM_EPS)
+    nu = list(cfg.get("nu", []))
+    d.n_freq = len(nu)
+    for i, v in enumerate(nu):
+        d.nu[i] = v
+    d.flow = cfg.get("flow", FLOW_TORUS if nu else FLOW_NONE)
+    d.torus_n0 = cfg.get("torus_n0", 1.0)
+    d.torus_kappa = cfg.get("torus_kappa", 1.0)
+    d.torus_hr = cfg.get("torus_hr", 0.3)
+    return d
+
+
+def n_data(cfg):
+    return 8 + 2 * len(cfg.get("nu", []))
+
+
+def trace(cfg, rays, nthreads=0):
+    """icond + every dump interval for the given ray indices.
+
+    Returns (states [n, n_data], info [n], steps [n])."""
+    L = lib()
+    d = make_desc(cfg)
+    rays = np.ascontiguousarray(rays, dtype=np.int64)
+    n = rays.size
+    out = np.zeros((n, n_data(cfg)))
+    info = np.zeros(n)
+    steps = np.zeros(n, dtype=np.int64)
+    rc = L.orc_trace(ctypes.byref(d), _pi(rays), n, _p(out), _p(info), _pi(steps), nthreads)
+    if rc != 0:
+        raise ValueError("oracle rejected the configuration")
+    return out, info, steps
+
+
+def icond(cfg, rays):
+    L = lib()
+    d = make_desc(cfg)
+    cam = np.zeros(4)
+    L.orc_camera(ctypes.byref(d), _p(cam))
+    out = np.zeros((len(rays), n_data(cfg)))
+    for k, r in enumerate(rays):
+        row = np.zeros(n_data(cfg))
+        L.orc_icond(ctypes.byref(d), _p(cam), int(r), _p(row))
+        out[k] = row
+    return out
+
+
+def ks_rhs(a, s):
+    s = np.ascontiguousarray(s, dtype=np.float64)
+    ds = np.zeros(8)
+    lib().orc_ks_rhs(a, _p(s), _p(ds))
+    return ds
+
+
+def rhs(cfg, s):
+    d = make_desc(cfg)
+    s = np.ascontiguousarray(s, dtype=np.float64)
+    ds = np.zeros_like(s)
+    lib().orc_rhs(ctypes.byref(d), _p(s), _p(ds))
+    return ds
+
+
+def integrate(cfg, s, dt):
+    d = make_desc(cfg)
+    s = np.array(s, dtype=np.float64)
+    lib().orc_integrate(ctypes.byref(d), _p(s), dt)
+    return s
+
+
+def down(a, q, u):
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    k = np.zeros(4)
+    lib().orc_down(a, _p(q), _p(u), _p(k))
+    return k
+
+
+def getuu(a, s):
+    s = np.ascontiguousarray(s, dtype=np.float64)
+    return lib().orc_getuu(a, _p(s))
+
+
+def getrr(a, q):
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    return lib().orc_getrr(a, _p(q))
+
+
+def getdt(cfg, q, dt):
+    d = make_desc(cfg)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    return lib().orc_getdt(ctypes.byref(d), _p(q), dt)
+
+
+def rplus(a):
+    return lib().orc_rplus(a)
+
+
+def risco(a):
+    return lib().orc_risco(a)
+
+
+def boosted_ks(m, a, v, axis, q):
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    out = np.zeros(50)
+    lib().orc_boosted_ks(m, a, v, axis, _p(q), _p(out))
+    return out
+
+
+# ---------------------------------------------------------------- grids
+
+class Grid:
+    """Keeps the numpy field arrays alive next to the OrcGrid struct."""
+
+    def __init__(self, fields, box, bug_gzz=False, physics=False):
+        self.fields = [np.ascontiguousarray(f, dtype=np.float32) for f in fields]
+        nz, ny, nx, nc = self.fields[0].shape
+        assert nc == 51
+        g = OrcGrid()
+        g.nx, g.ny, g.nz = nx, ny, nz
+        for i in range(8):
+            g.box[i] = box[i]
+        g.fields[0] = self.fields[0].ctypes.data
+        g.fields[1] = self.fields[-1].ctypes.data
+        g.bug_gzz = int(bug_gzz)
+        g.physics = int(physics)
+        self.g = g
+
+
+def fisheye_nodes(lo, hi, n):
+    """Fisheye node coordinates x = sinh((A i + B)^3) (tools/generate_data.py:49-58)."""
+    B = np.cbrt(np.arcsinh(lo))
+    A = (np.cbrt(np.arcsinh(hi)) - B) / (n - 1)
+    f = A * np.arange(n) + B
+    return np.sinh(f * f * f)
+
+
+def boosted_ks_grid(n, lo, hi, t, m=1.0, a=0.7, v=0.3, axis=1, rho=True):
+    """Sample the boosted KS fields on an n^3 fisheye grid (slow, for small n)."""
+    xs = fisheye_nodes(lo, hi, n)
+    out = np.zeros((n, n, n, 51), dtype=np.float64)
+    L = lib()
+    q = np.zeros(4)
+    buf = np.zeros(50)
+    for k, z in enumerate(xs):
+        for j, y in enumerate(xs):
+            for i, x in enumerate(xs):
+                q[:] = (t, x, y, z)
+                L.orc_boosted_ks(m, a, v, axis, _p(q), _p(buf))
+                out[k, j, i, :50] = buf
+                out[k, j, i, 50] = 1.0 / np.sqrt(x * x + y * y + z * z) if rho else 0.0
+    out = np.nan_to_num(out)
+    return out.astype(np.float32)
+
+
+def dyst_rhs(grid, s):
+    s = np.ascontiguousarray(s, dtype=np.float64)
+    ds = np.zeros(8)
+    lib().orc_dyst_rhs(ctypes.byref(grid.g), _p(s), _p(ds))
+    return ds
+
+
+def dyst_trace(cfg, grid, rays, nthreads=0):
+    L = lib()
+    d = make_desc(cfg)
+    rays = np.ascontiguousarray(rays, dtype=np.int64)
+    n = rays.size
+    out = np.zeros((n, 8))
+    info = np.zeros(n)
+    steps = np.zeros(n, dtype=np.int64)
+    L.orc_dyst_trace(ctypes.byref(d), ctypes.byref(grid.g), _pi(rays), n, _p(out),
+                     _p(info), _pi(steps), nthreads)
+    return out, info, steps

@@ -1,0 +1,54 @@
+"""CPU-side checks of the C ABI: the library loads and exports exactly
+what include/gray_cuda.h declares; argument validation needs no GPU."""
+import ctypes
+import os
+import re
+
+from gray_b200 import api
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions(path):
+    src = open(path).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"\b(gray_[a-z0-9_]+)\s*\(", src)
+    return sorted(set(names))
+
+
+def test_header_matches_python_export_list():
+    assert header_functions(os.path.join(ROOT, "include", "gray_cuda.h")) == sorted(api.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol():
+    L = api.lib()
+    for name in header_functions(os.path.join(ROOT, "include", "gray_cuda.h")):
+        assert hasattr(L, name), name
+
+
+def test_strerror_and_version():
+    assert api.lib().gray_abi_version() == 1
+    assert api.strerror(api.EINVAL).startswith("invalid")
+    assert api.strerror(api.EBUDGET).startswith("request exceeds")
+    assert api.strerror(12345) == "unknown status"
+
+
+def test_null_context_is_rejected():
+    L = api.lib()
+    assert L.gray_sync(None) == api.EINVAL
+    assert L.gray_set_stream(None, None) == api.EINVAL
+    rid = ctypes.c_int(0)
+    d = api.make_desc({})
+    assert L.gray_render_create(None, ctypes.byref(d), ctypes.byref(rid)) == api.EINVAL
+    assert L.gray_icond(None, 1) == api.ENOTFOUND
+    assert L.gray_hbm_used(None) == 0
+
+
+def test_desc_defaults_follow_reference_opts():
+    d = api.make_desc({})
+    # sim/Kerr.opts, sim/infcam.opts, sim/gray.opts, sim-org/setup.opts
+    assert (d.m_bh, d.a_spin) == (4e6, 0.0)
+    assert (d.w_img, d.h_img, d.r_obs, d.i_obs, d.j_obs) == (64.0, 64.0, 1024.0, 60.0, 0.0)
+    assert (d.n_width, d.n_height) == (512, 512)
+    assert (d.t_init, d.dt_dump, d.n_dump, d.n_sub) == (0.0, -32.0, 64, 1024)
+    assert d.n_freq == 0 and d.flow == api.FLOW_NONE
