@@ -31,7 +31,9 @@ EXPORTS = [
     "gray_read_state", "gray_write_state", "gray_read_kdown", "gray_ray_steps",
     "gray_load_spacetime", "gray_load_spacetime_interleaved",
     "gray_make_boosted_ks", "gray_swap_levels", "gray_measure_peak",
+    "gray_run_mixed_noalloc",
 ]
+NOALLOC_MAX_RENDERS = 32
 
 
 class GrayError(RuntimeError):
@@ -134,6 +136,7 @@ def lib():
         L.gray_make_boosted_ks.argtypes = [vp, P(GridDesc), d, d, i, d, i]
         L.gray_swap_levels.argtypes = [vp]
         L.gray_measure_peak.argtypes = [vp, i, P(d)]
+        L.gray_run_mixed_noalloc.argtypes = [i, P(RenderDesc), i, P(vp), P(vp), vp, P(u64)]
         _lib = L
     return _lib
 

@@ -216,6 +216,19 @@ grid_ready(gray_ctx *c)
 
 } /* namespace */
 
+/* Shared with other translation units through gray_internal.h. */
+int
+gray_internal_check_desc(const gray_render_desc *d)
+{
+	return check_desc(d);
+}
+
+void
+gray_internal_make_params(const gray_render_desc *d, RenderParams *p)
+{
+	make_params(d, p);
+}
+
 /* ------------------------------------------------------------------------ */
 
 extern "C" const char *

@@ -47,6 +47,10 @@ struct GridParams {
 	int    single;           /* t1 == t2: use level 0 only               */
 };
 
+/* descriptor validation and per-render constants (gray_api.cu) */
+int  gray_internal_check_desc(const gray_render_desc *d);
+void gray_internal_make_params(const gray_render_desc *d, RenderParams *p);
+
 /* ---- launchers (one per translation unit) ---- */
 cudaError_t launch_icond64(const RenderParams &p, double *data, double *info,
                            cudaStream_t st);

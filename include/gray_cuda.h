@@ -192,6 +192,35 @@ int gray_make_boosted_ks(gray_ctx *ctx, const gray_grid_desc *grid, double a,
 /* Swap the two time levels (io.c:279-300 copy_snapshot). */
 int gray_swap_levels(gray_ctx *ctx);
 
+/* ---- allocation-free entry point ----------------------------------- */
+
+/* No counterpart in the reference.  For callers that cannot call
+ * cudaMalloc -- hosts whose own allocator already owns the device memory
+ * and forbids side allocations, or latency-critical loops that cannot take
+ * the device-wide synchronisation cudaMalloc/cudaFree imply -- this runs
+ * gray_icond + gray_evolve_all of up to GRAY_NOALLOC_MAX_RENDERS analytic
+ * Kerr-Schild renders in mixed precision without allocating anything.
+ *
+ *  - state_dev[i] / info_dev[i]: device buffers the caller owns, of
+ *    n_width*n_height*(8 + 2 n_freq) and n_width*n_height doubles (SoA,
+ *    as gray_read_state returns them); they are written.
+ *  - All renders of one call share n_freq and flow; rays over all renders
+ *    must not exceed 2^31.  More renders, or more rays, return GRAY_EINVAL.
+ *  - The kernel's scratch (render table, ray queue, step counter:
+ *    GRAY_NOALLOC_SCRATCH_BYTES) is a static device array that every GPU
+ *    loading this library holds until exit.  The first call on a device
+ *    looks up its address (cudaGetSymbolAddress); make that first call
+ *    before any stream capture.  Every call shares the array: calls that
+ *    overlap on the GPU (other streams, other host threads) race.
+ *  - Work is enqueued on cuda_stream (a cudaStream_t, NULL = legacy default
+ *    stream).  If steps_host is non-NULL the call waits and stores the
+ *    accepted ray-steps there; otherwise it returns after enqueueing. */
+#define GRAY_NOALLOC_MAX_RENDERS   32
+#define GRAY_NOALLOC_SCRATCH_BYTES 8192
+int gray_run_mixed_noalloc(int device, const gray_render_desc *descs, int n_renders,
+                           double *const *state_dev, double *const *info_dev,
+                           void *cuda_stream, uint64_t *steps_host);
+
 /* ---- measurement (no reference counterpart) ------------------------ */
 
 /* CUDA-core FMA-loop peak of the context's device in FLOP/s (FMA = 2):
