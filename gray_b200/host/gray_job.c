@@ -1,0 +1,486 @@
+/*
+ * The GRay2 lux job in C, driving libgray_cuda.
+ *
+ * Options: the union of the reference's run-time tables, same names,
+ * aliases and defaults --
+ *   sim/gray.opts:1-14      i_platform:ip i_device:id device_type:type
+ *                           spacetime:st initcond:ic t_init:t0 dt_dump:dt
+ *                           i_init:i0 n_dump:N rayfile:ray
+ *   sim/Kerr.opts:1-2       m_bh:M a_spin:a
+ *   sim/infcam.opts:2-11    w_img:w h_img:h r_obs:r i_obs:i j_obs:j
+ *                           coordinates:coor n_width:W n_height:H
+ *   sim-org/setup.opts:6-15 precision:p scheme:scm morder:mo:ml kflags:kf
+ *                           outfile:out n_sub:n
+ *   sim-org/param.opts:4-18 M_ADM:m dyst_file:data enable_fast_light:fast_light
+ *                           n_electron:ne beta_crit:bc R_high:Rh R_low:Rl nu
+ * plus the options of the analytic torus (flow, torus_n0, torus_kappa,
+ * torus_hr) and the stop rule (term).  conf() follows the lux convention:
+ * 0 when the argument was consumed (sim/gray.c:37-73).
+ *
+ * init() replaces sim/gray.c:75-151 (device, ray buffer, initcond, planner);
+ * exec() replaces the dump loop of sim-org/gray.c:243-294 with the per-dump
+ * evolve the new tree leaves as a TODO (sim/gray.c:168), and writes the raw
+ * dumps of sim-org/io.c:39-72.
+ */
+#include "gray_job.h"
+
+#include <errno.h>
+#include <math.h>
+#include <stddef.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef enum { T_DBL, T_SIZE, T_UINT, T_STR, T_LIST, T_PREC } opt_type;
+
+struct gray_job {
+	gray_lux_job super;
+
+	/* sim/gray.opts */
+	unsigned i_platform, i_device;
+	char     device_type[32];
+	char     spacetime[32];
+	char     initcond[32];
+	double   t_init, dt_dump;
+	size_t   i_init, n_dump;
+	char     rayfile[256];
+	/* sim/Kerr.opts */
+	double   m_bh, a_spin;
+	/* sim/infcam.opts */
+	double   w_img, h_img, r_obs, i_obs, j_obs;
+	char     coordinates[32];
+	size_t   n_width, n_height;
+	/* sim-org/setup.opts */
+	int      precision;          /* size of real: 4 (mixed here) or 8 */
+	char     scheme[16];
+	char     morder[16];
+	char     kflags[64];
+	char     outfile[256];
+	size_t   n_sub;
+	/* sim-org/param.opts */
+	double   M_ADM;
+	char     dyst_file[256];
+	size_t   enable_fast_light;
+	double   n_electron, beta_crit, R_high, R_low;
+	double   nu[GRAY_MAX_FREQ];
+	int      n_freq;
+	/* analytic torus and stop rule */
+	char     flow[16];
+	double   torus_n0, torus_kappa, torus_hr;
+	char     term[16];
+
+	/* run time */
+	gray_ctx *ctx;
+	int       render;
+	uint64_t  steps;
+	double    ns;
+};
+
+#define EGO ((struct gray_job *)ego)
+#define OFF(f) offsetof(struct gray_job, f)
+#define SZ(f)  sizeof(((struct gray_job *)0)->f)
+
+typedef struct {
+	const char *names;   /* "name:alias:alias" */
+	opt_type    type;
+	size_t      off, size;
+	const char *dflt;
+} opt;
+
+static const opt OPTS[] = {
+	{"i_platform:ip",        T_UINT, OFF(i_platform), SZ(i_platform), "0"},
+	{"i_device:id",          T_UINT, OFF(i_device), SZ(i_device), "0"},
+	{"device_type:type",     T_STR,  OFF(device_type), SZ(device_type), "all"},
+	{"spacetime:st",         T_STR,  OFF(spacetime), SZ(spacetime), "Kerr"},
+	{"initcond:ic",          T_STR,  OFF(initcond), SZ(initcond), "infcam"},
+	{"t_init:t0",            T_DBL,  OFF(t_init), SZ(t_init), "0"},
+	{"dt_dump:dt",           T_DBL,  OFF(dt_dump), SZ(dt_dump), "-32"},
+	{"i_init:i0",            T_SIZE, OFF(i_init), SZ(i_init), "0"},
+	{"n_dump:N",             T_SIZE, OFF(n_dump), SZ(n_dump), "64"},
+	{"rayfile:ray",          T_STR,  OFF(rayfile), SZ(rayfile), "ray%04d.h5"},
+	{"m_bh:M",               T_DBL,  OFF(m_bh), SZ(m_bh), "4e6"},
+	{"a_spin:a",             T_DBL,  OFF(a_spin), SZ(a_spin), "0"},
+	{"w_img:w",              T_DBL,  OFF(w_img), SZ(w_img), "64"},
+	{"h_img:h",              T_DBL,  OFF(h_img), SZ(h_img), "64"},
+	{"r_obs:r",              T_DBL,  OFF(r_obs), SZ(r_obs), "1024"},
+	{"i_obs:i",              T_DBL,  OFF(i_obs), SZ(i_obs), "60"},
+	{"j_obs:j",              T_DBL,  OFF(j_obs), SZ(j_obs), "0"},
+	{"coordinates:coor",     T_STR,  OFF(coordinates), SZ(coordinates), "pxcenter"},
+	{"n_width:W:w_rays",     T_SIZE, OFF(n_width), SZ(n_width), "512"},
+	{"n_height:H:h_rays",    T_SIZE, OFF(n_height), SZ(n_height), "512"},
+	{"precision:p",          T_PREC, OFF(precision), SZ(precision), "4"},
+	{"scheme:scm",           T_STR,  OFF(scheme), SZ(scheme), "RK4"},
+	{"morder:mo:ml",         T_STR,  OFF(morder), SZ(morder), "AoS"},
+	{"kflags:kf",            T_STR,  OFF(kflags), SZ(kflags), "-w"},
+	{"outfile:out",          T_STR,  OFF(outfile), SZ(outfile), "%04d.raw"},
+	{"n_sub:n",              T_SIZE, OFF(n_sub), SZ(n_sub), "1024"},
+	{"M_ADM:m",              T_DBL,  OFF(M_ADM), SZ(M_ADM), "4.3e6"},
+	{"dyst_file:data",       T_STR,  OFF(dyst_file), SZ(dyst_file), "data.h5"},
+	{"enable_fast_light:fast_light", T_SIZE, OFF(enable_fast_light), SZ(enable_fast_light), "0"},
+	{"n_electron:ne",        T_DBL,  OFF(n_electron), SZ(n_electron), "1e6"},
+	{"beta_crit:bc",         T_DBL,  OFF(beta_crit), SZ(beta_crit), "1"},
+	{"R_high:Rh",            T_DBL,  OFF(R_high), SZ(R_high), "1"},
+	{"R_low:Rl",             T_DBL,  OFF(R_low), SZ(R_low), "1"},
+	{"nu",                   T_LIST, OFF(nu), SZ(nu), ""},
+	{"flow",                 T_STR,  OFF(flow), SZ(flow), "torus"},
+	{"torus_n0",             T_DBL,  OFF(torus_n0), SZ(torus_n0), "1"},
+	{"torus_kappa",          T_DBL,  OFF(torus_kappa), SZ(torus_kappa), "1"},
+	{"torus_hr",             T_DBL,  OFF(torus_hr), SZ(torus_hr), "0.3"},
+	{"term",                 T_STR,  OFF(term), SZ(term), "eps"},
+};
+#define N_OPTS (sizeof(OPTS) / sizeof(OPTS[0]))
+
+/* name matches one of the ':'-separated names of o */
+static int
+matches(const opt *o, const char *name, size_t len)
+{
+	const char *p = o->names;
+	while(*p) {
+		const char *e = strchr(p, ':');
+		size_t n = e ? (size_t)(e - p) : strlen(p);
+		if(n == len && strncmp(p, name, len) == 0)
+			return 1;
+		if(!e)
+			break;
+		p = e + 1;
+	}
+	return 0;
+}
+
+/* parse a full double; the whole token must be consumed */
+static int
+parse_dbl(const char *s, double *v)
+{
+	char *rem;
+	errno = 0;
+	*v = strtod(s, &rem);
+	return (rem == s || *rem != '\0' || errno == ERANGE) ? GRAY_EINVAL : GRAY_OK;
+}
+
+static int
+parse_size(const char *s, size_t *v)
+{
+	char *rem;
+	if(*s == '-')
+		return GRAY_EINVAL;
+	errno = 0;
+	unsigned long long x = strtoull(s, &rem, 0);
+	if(rem == s || *rem != '\0' || errno == ERANGE)
+		return GRAY_EINVAL;
+	*v = (size_t)x;
+	return GRAY_OK;
+}
+
+/* strtoprec of setup.opts: "4"/"single"/"float" or "8"/"double"; "mixed"
+ * names the FP32-bulk path, which is what the single-precision request
+ * runs here. */
+static int
+parse_prec(const char *s, int *v)
+{
+	if(!strcmp(s, "4") || !strcmp(s, "single") || !strcmp(s, "float") || !strcmp(s, "mixed"))
+		*v = 4;
+	else if(!strcmp(s, "8") || !strcmp(s, "double"))
+		*v = 8;
+	else
+		return GRAY_EINVAL;
+	return GRAY_OK;
+}
+
+/* strtoda of param.opts:18: a comma-separated list of reals; empty or
+ * "none" turns transfer off (the reference's NaN-terminated empty list). */
+static int
+parse_list(const char *s, double *v, int *n)
+{
+	int k = 0;
+	char buf[512];
+	if(!*s || !strcmp(s, "none")) {
+		*n = 0;
+		return GRAY_OK;
+	}
+	if(strlen(s) >= sizeof(buf))
+		return GRAY_EINVAL;
+	strcpy(buf, s);
+	for(char *tok = strtok(buf, ","); tok; tok = strtok(NULL, ",")) {
+		double x;
+		if(k == GRAY_MAX_FREQ || parse_dbl(tok, &x) || !(x > 0.0))
+			return GRAY_EINVAL;
+		v[k++] = x;
+	}
+	*n = k;
+	return GRAY_OK;
+}
+
+static int
+set_opt(struct gray_job *j, const opt *o, const char *val)
+{
+	void *dst = (char *)j + o->off;
+	switch(o->type) {
+	case T_DBL: {
+		double v;
+		if(parse_dbl(val, &v))
+			return GRAY_EINVAL;
+		*(double *)dst = v;
+		return GRAY_OK;
+	}
+	case T_SIZE: {
+		size_t v;
+		if(parse_size(val, &v))
+			return GRAY_EINVAL;
+		*(size_t *)dst = v;
+		return GRAY_OK;
+	}
+	case T_UINT: {
+		size_t v;
+		if(parse_size(val, &v) || v > 0xffffffffu)
+			return GRAY_EINVAL;
+		*(unsigned *)dst = (unsigned)v;
+		return GRAY_OK;
+	}
+	case T_STR:
+		if(strlen(val) >= o->size)
+			return GRAY_EINVAL;
+		strcpy((char *)dst, val);
+		return GRAY_OK;
+	case T_LIST:
+		return parse_list(val, (double *)dst, &j->n_freq);
+	case T_PREC:
+		return parse_prec(val, (int *)dst);
+	}
+	return GRAY_EINVAL;
+}
+
+static int
+valid_choices(const struct gray_job *j)
+{
+	if(strcmp(j->spacetime, "Kerr") && strcmp(j->spacetime, "KS"))
+		return 0; /* sim/gray.c:55-57: unknown spacetime */
+	if(strcmp(j->initcond, "infcam"))
+		return 0; /* sim/gray.c:67-69: unknown initial conditions */
+	if(strcmp(j->scheme, "RK4"))
+		return 0; /* sim-org/setup.opts:7: the only scheme shipped */
+	if(strcmp(j->morder, "AoS") && strcmp(j->morder, "SoA"))
+		return 0;
+	if(strcmp(j->flow, "torus") && strcmp(j->flow, "none"))
+		return 0;
+	if(strcmp(j->term, "eps") && strcmp(j->term, "rplus"))
+		return 0;
+	return 1;
+}
+
+static int
+conf(gray_lux_job *ego, const char *arg)
+{
+	const char *eq = arg ? strchr(arg, '=') : NULL;
+	if(!eq)
+		return GRAY_JOB_UNKNOWN;
+	for(size_t k = 0; k < N_OPTS; ++k) {
+		if(!matches(&OPTS[k], arg, (size_t)(eq - arg)))
+			continue;
+		struct gray_job save = *EGO;
+		int st = set_opt(EGO, &OPTS[k], eq + 1);
+		if(st == GRAY_OK && !valid_choices(EGO))
+			st = GRAY_EINVAL;
+		if(st != GRAY_OK)
+			*EGO = save; /* a rejected value leaves the job unchanged */
+		return st;
+	}
+	return GRAY_JOB_UNKNOWN;
+}
+
+int
+gray_job_desc(const gray_lux_job *ego, gray_render_desc *d)
+{
+	if(!ego || !d)
+		return GRAY_EINVAL;
+	const struct gray_job *j = (const struct gray_job *)ego;
+	memset(d, 0, sizeof(*d));
+	d->m_bh = j->m_bh;
+	d->a_spin = j->a_spin;
+	d->w_img = j->w_img;
+	d->h_img = j->h_img;
+	d->r_obs = j->r_obs;
+	d->i_obs = j->i_obs;
+	d->j_obs = j->j_obs;
+	d->n_width = j->n_width;
+	d->n_height = j->n_height;
+	d->t_init = j->t_init;
+	d->dt_dump = j->dt_dump;
+	d->n_sub = j->n_sub;
+	d->n_dump = j->n_dump;
+	d->term = strcmp(j->term, "rplus") ? GRAY_TERM_EPS : GRAY_TERM_RPLUS;
+	d->n_freq = j->n_freq;
+	for(int i = 0; i < j->n_freq; ++i)
+		d->nu[i] = j->nu[i];
+	d->flow = (j->n_freq && !strcmp(j->flow, "torus")) ? GRAY_FLOW_TORUS : GRAY_FLOW_NONE;
+	d->torus_n0 = j->torus_n0;
+	d->torus_kappa = j->torus_kappa;
+	d->torus_hr = j->torus_hr;
+	d->spacetime = GRAY_ST_KERR;
+	d->precision = j->precision == 8 ? GRAY_PREC_FP64 : GRAY_PREC_MIXED;
+	return GRAY_OK;
+}
+
+int
+gray_job_get(const gray_lux_job *ego, const char *name, char *buf, size_t len)
+{
+	if(!ego || !name || !buf || !len)
+		return GRAY_EINVAL;
+	const struct gray_job *j = (const struct gray_job *)ego;
+	for(size_t k = 0; k < N_OPTS; ++k) {
+		const opt *o = &OPTS[k];
+		if(!matches(o, name, strlen(name)))
+			continue;
+		const void *src = (const char *)j + o->off;
+		int n = 0;
+		switch(o->type) {
+		case T_DBL:  n = snprintf(buf, len, "%.17g", *(const double *)src); break;
+		case T_SIZE: n = snprintf(buf, len, "%zu", *(const size_t *)src); break;
+		case T_UINT: n = snprintf(buf, len, "%u", *(const unsigned *)src); break;
+		case T_STR:  n = snprintf(buf, len, "%s", (const char *)src); break;
+		case T_PREC: n = snprintf(buf, len, "%d", *(const int *)src); break;
+		case T_LIST: {
+			size_t used = 0;
+			buf[0] = '\0';
+			for(int i = 0; i < j->n_freq && used < len; ++i)
+				used += (size_t)snprintf(buf + used, len - used, i ? ",%.17g" : "%.17g", j->nu[i]);
+			n = (int)used;
+			break;
+		}
+		}
+		return (n < 0 || (size_t)n >= len) ? GRAY_ESIZE : GRAY_OK;
+	}
+	return GRAY_ENOTFOUND;
+}
+
+int
+gray_job_stats(const gray_lux_job *ego, uint64_t *ray_steps, double *kernel_ns)
+{
+	if(!ego)
+		return GRAY_EINVAL;
+	if(ray_steps)
+		*ray_steps = EGO->steps;
+	if(kernel_ns)
+		*kernel_ns = EGO->ns;
+	return GRAY_OK;
+}
+
+int
+gray_write_raw(const char *path, const double *data, const double *info,
+               size_t n_data, size_t w, size_t h)
+{
+	const size_t sz = sizeof(double), n_rays = w * h, n_info = 1;
+	FILE *f = fopen(path, "wb");
+	if(!f)
+		return GRAY_EINVAL;
+	int ok = fwrite(&sz, sizeof(size_t), 1, f) == 1 &&
+	         fwrite(&n_data, sizeof(size_t), 1, f) == 1 &&
+	         fwrite(&w, sizeof(size_t), 1, f) == 1 &&
+	         fwrite(&h, sizeof(size_t), 1, f) == 1 &&
+	         fwrite(data, sz * n_data, n_rays, f) == n_rays &&
+	         fwrite(info, sz * n_info, n_rays, f) == n_rays;
+	return (fclose(f) == 0 && ok) ? GRAY_OK : GRAY_EINVAL;
+}
+
+/* sim-org/io.c:39-72 dump(): state in AoS with its info diagnostic */
+static int
+dump(struct gray_job *j, size_t i)
+{
+	if(!j->outfile[0])
+		return GRAY_OK; /* dumps switched off */
+	gray_render_desc d;
+	gray_job_desc(&j->super, &d);
+	const size_t n_rays = d.n_width * d.n_height;
+	const size_t n_data = 8 + 2 * (size_t)d.n_freq;
+	double *data = malloc(sizeof(double) * n_rays * n_data);
+	double *info = malloc(sizeof(double) * n_rays);
+	int st = (data && info) ? GRAY_OK : GRAY_ENOMEM;
+	if(!st)
+		st = gray_read_state(j->ctx, j->render, data, sizeof(double) * n_rays * n_data,
+		                     info, sizeof(double) * n_rays, GRAY_LAYOUT_AOS);
+	if(!st) {
+		char name[512];
+		snprintf(name, sizeof(name), j->outfile, (int)i);
+		st = gray_write_raw(name, data, info, n_data, d.n_width, d.n_height);
+	}
+	free(data);
+	free(info);
+	return st;
+}
+
+static int
+init(gray_lux_job *ego)
+{
+	gray_render_desc d;
+	int st;
+	printf("GRay2:init: spacetime:st: %s, initcond:ic: %s\n", EGO->spacetime, EGO->initcond);
+	gray_job_desc(ego, &d);
+	EGO->ctx = gray_create((int)EGO->i_device, 0, &st);
+	if(!EGO->ctx)
+		return st;
+	st = gray_render_create(EGO->ctx, &d, &EGO->render);
+	if(st)
+		return st;
+	EGO->steps = 0;
+	EGO->ns = 0.0;
+	return GRAY_OK;
+}
+
+/* sim-org/gray.c:243-294 */
+static int
+exec(gray_lux_job *ego)
+{
+	struct gray_job *j = EGO;
+	size_t i = j->i_init;
+	if(!j->ctx)
+		return GRAY_ESTATE;
+	const double n_rays = (double)j->n_width * (double)j->n_height;
+	int st = gray_icond(j->ctx, j->render);
+	if(st)
+		return st;
+	printf("%zu:  initialize at %4.1f", i, j->t_init);
+	if((st = dump(j, i)))
+		return st;
+	printf(": DONE\n");
+	while(i < j->n_dump) {
+		double ns;
+		double t      = j->t_init + (double)i * j->dt_dump;
+		double target = j->t_init + (double)(++i) * j->dt_dump;
+		printf("%zu: %4.1f -> %4.1f", i, t, target);
+		if((st = gray_evolve(j->ctx, j->render, t, target, j->n_sub, &ns)))
+			return st;
+		if((st = dump(j, i)))
+			return st;
+		j->ns += ns;
+		printf(": DONE (%.3gns/step/ray)\n", ns / (double)j->n_sub / n_rays);
+	}
+	fflush(stdout);
+	return gray_ray_steps(j->ctx, j->render, &j->steps);
+}
+
+gray_lux_job *
+gray_job_mkmod(const void *opts)
+{
+	(void)opts;
+	struct gray_job *j = calloc(1, sizeof(*j));
+	if(!j)
+		return NULL;
+	for(size_t k = 0; k < N_OPTS; ++k)
+		if(set_opt(j, &OPTS[k], OPTS[k].dflt) != GRAY_OK) {
+			free(j);
+			return NULL;
+		}
+	j->super.conf = conf;
+	j->super.init = init;
+	j->super.exec = exec;
+	return &j->super;
+}
+
+void
+gray_job_rmmod(gray_lux_job *ego)
+{
+	if(!ego)
+		return;
+	if(EGO->ctx)
+		gray_destroy(EGO->ctx); /* frees the render as well */
+	free(ego);
+}

@@ -1,0 +1,151 @@
+"""The lux-job surface in C (gray_b200/host/gray_job.c): option names,
+aliases and defaults of the reference's .opts tables, conf() semantics, the
+raw dump format of sim-org/io.c:39-72, and (GPU) the `gray` CLI against the
+oracle."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+from gray_b200 import api
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "gray_b200", "lib", "libgray_job.so")
+CLI = os.path.join(ROOT, "gray_b200", "lib", "gray")
+UNKNOWN = 1
+
+
+class Job:
+    def __init__(self):
+        api.lib()  # libgray_cuda.so first (libgray_job.so links to it)
+        L = ctypes.CDLL(LIB)
+        L.gray_job_mkmod.restype = ctypes.c_void_p
+        L.gray_job_mkmod.argtypes = [ctypes.c_void_p]
+        L.gray_job_rmmod.argtypes = [ctypes.c_void_p]
+        L.gray_job_desc.argtypes = [ctypes.c_void_p, ctypes.POINTER(api.RenderDesc)]
+        L.gray_job_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t]
+        L.gray_write_raw.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t]
+        self.L = L
+        self.h = L.gray_job_mkmod(None)
+        assert self.h
+        CONF = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_char_p)
+        # struct gray_lux_job: the vtable is the first member
+        self.conf_fn = CONF(ctypes.cast(self.h, ctypes.POINTER(ctypes.c_void_p))[0])
+
+    def conf(self, arg):
+        return self.conf_fn(self.h, arg.encode())
+
+    def get(self, name):
+        buf = ctypes.create_string_buffer(512)
+        assert self.L.gray_job_get(self.h, name.encode(), buf, 512) == 0
+        return buf.value.decode()
+
+    def desc(self):
+        d = api.RenderDesc()
+        assert self.L.gray_job_desc(self.h, ctypes.byref(d)) == 0
+        return d
+
+    def close(self):
+        self.L.gray_job_rmmod(self.h)
+
+
+@pytest.fixture
+def job():
+    j = Job()
+    yield j
+    j.close()
+
+
+def test_defaults_are_the_reference_opts(job):
+    expect = {
+        # sim/gray.opts
+        "i_platform": "0", "i_device": "0", "spacetime": "Kerr", "initcond": "infcam",
+        "t_init": "0", "dt_dump": "-32", "i_init": "0", "n_dump": "64", "rayfile": "ray%04d.h5",
+        # sim/Kerr.opts
+        "m_bh": "4000000", "a_spin": "0",
+        # sim/infcam.opts
+        "w_img": "64", "h_img": "64", "r_obs": "1024", "i_obs": "60", "j_obs": "0",
+        "coordinates": "pxcenter", "n_width": "512", "n_height": "512",
+        # sim-org/setup.opts
+        "precision": "4", "scheme": "RK4", "morder": "AoS", "kflags": "-w",
+        "outfile": "%04d.raw", "n_sub": "1024",
+        # sim-org/param.opts
+        "M_ADM": "4300000", "dyst_file": "data.h5", "enable_fast_light": "0",
+        "n_electron": "1000000", "beta_crit": "1", "R_high": "1", "R_low": "1", "nu": "",
+    }
+    for k, v in expect.items():
+        assert job.get(k) == v, k
+
+
+def test_aliases_and_values(job):
+    for arg in ["a=0.9", "M=10", "w=40", "h=30", "r=1000", "i=17", "j=5", "W=96", "H=48",
+                "t0=1", "dt=-31.25", "i0=0", "N=7", "n=1000", "p=8", "mo=SoA", "ml=AoS",
+                "st=KS", "ic=infcam", "id=0", "ip=0", "type=gpu", "out=", "nu=1,2,4,8",
+                "torus_kappa=125.8988", "term=rplus"]:
+        assert job.conf(arg) == 0, arg
+    d = job.desc()
+    assert (d.a_spin, d.m_bh, d.w_img, d.h_img, d.r_obs, d.i_obs, d.j_obs) == (0.9, 10, 40, 30, 1000, 17, 5)
+    assert (d.n_width, d.n_height, d.n_dump, d.n_sub) == (96, 48, 7, 1000)
+    assert (d.t_init, d.dt_dump) == (1.0, -31.25)
+    assert d.precision == api.PREC_FP64
+    assert d.n_freq == 4 and list(d.nu)[:4] == [1, 2, 4, 8] and d.flow == api.FLOW_TORUS
+    assert d.term == api.TERM_RPLUS
+    assert job.get("nu") == "1,2,4,8"
+    assert job.get("outfile") == ""
+    assert job.conf("p=single") == 0 and job.desc().precision == api.PREC_MIXED
+
+
+def test_conf_rejects_without_side_effects(job):
+    assert job.conf("bogus=1") == UNKNOWN
+    assert job.conf("no_equals_sign") == UNKNOWN
+    assert job.conf("a=0.3") == 0
+    for bad in ["a=abc", "a=", "N=-1", "W=1x", "st=Minkowski", "ic=pinhole", "scm=RK45",
+                "p=16", "nu=1,-2", "nu=1,2,3,4,5,6,7,8,9", "flow=disk"]:
+        assert job.conf(bad) == api.EINVAL, bad
+    assert job.get("a_spin") == "0.29999999999999999"
+    assert job.get("spacetime") == "Kerr"
+
+
+def test_raw_dump_format(job, tmp_path):
+    """sim-org/io.c:58-67: {sz, n_data, W, H} as size_t, data, info."""
+    w, h, nd = 5, 3, 10
+    data = np.arange(w * h * nd, dtype=np.float64).reshape(w * h, nd)
+    info = -np.arange(w * h, dtype=np.float64)
+    path = str(tmp_path / "0007.raw")
+    assert job.L.gray_write_raw(path.encode(), data.ctypes.data, info.ctypes.data, nd, w, h) == 0
+    raw = open(path, "rb").read()
+    hdr = np.frombuffer(raw[:32], dtype=np.uint64)
+    assert list(hdr) == [8, nd, w, h]
+    body = np.frombuffer(raw[32:], dtype=np.float64)
+    assert np.array_equal(body[: w * h * nd].reshape(w * h, nd), data)
+    assert np.array_equal(body[w * h * nd:], info)
+
+
+def read_raw(path):
+    raw = open(path, "rb").read()
+    sz, nd, w, h = (int(x) for x in np.frombuffer(raw[:32], dtype=np.uint64))
+    body = np.frombuffer(raw[32:], dtype=np.float64)
+    return body[: w * h * nd].reshape(w * h, nd), body[w * h * nd:]
+
+
+@pytest.mark.gpu
+def test_cli_dumps_match_oracle(tmp_path):
+    args = ["a=0.9", "r=1000", "i=60", "w=40", "h=40", "W=12", "H=10", "dt=-31.25",
+            "n=1000", "N=3", "p=8", "out=" + str(tmp_path / "%04d.raw")]
+    res = subprocess.run([CLI] + args, capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stderr
+    assert "3: -62.5 -> -93.8: DONE" in res.stdout
+    cfg = dict(a_spin=0.9, r_obs=1000.0, i_obs=60.0, w_img=40.0, h_img=40.0, n_width=12,
+               n_height=10, dt_dump=-31.25, n_sub=1000)
+    for i in range(4):
+        data, info = read_raw(str(tmp_path / ("%04d.raw" % i)))
+        if i == 0:
+            ref = O.icond(cfg, range(120))
+        else:
+            ref, _, _ = O.trace(dict(cfg, n_dump=i), np.arange(120))
+        assert np.array_equal(data, ref), i
+        assert np.max(np.abs(info)) < 1e-9
