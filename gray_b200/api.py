@@ -31,7 +31,7 @@ EXPORTS = [
     "gray_read_state", "gray_write_state", "gray_read_kdown", "gray_ray_steps",
     "gray_load_spacetime", "gray_load_spacetime_interleaved",
     "gray_make_boosted_ks", "gray_swap_levels", "gray_measure_peak",
-    "gray_run_mixed_noalloc",
+    "gray_run_mixed_noalloc", "gray_read_spacetime",
 ]
 NOALLOC_MAX_RENDERS = 32
 
@@ -137,6 +137,7 @@ def lib():
         L.gray_swap_levels.argtypes = [vp]
         L.gray_measure_peak.argtypes = [vp, i, P(d)]
         L.gray_run_mixed_noalloc.argtypes = [i, P(RenderDesc), i, P(vp), P(vp), vp, P(u64)]
+        L.gray_read_spacetime.argtypes = [vp, i, vp, sz]
         _lib = L
     return _lib
 
@@ -272,6 +273,12 @@ class Context:
         v = ctypes.c_double(0.0)
         _ck(lib().gray_measure_peak(self.h, precision, ctypes.byref(v)), "gray_measure_peak")
         return v.value
+
+    def read_spacetime(self, grid, level):
+        out = np.empty((grid.nz, grid.ny, grid.nx, 51), dtype=np.float32)
+        _ck(lib().gray_read_spacetime(self.h, level, out.ctypes.data, out.nbytes),
+            "gray_read_spacetime")
+        return out
 
     def swap_levels(self):
         _ck(lib().gray_swap_levels(self.h), "gray_swap_levels")

@@ -463,7 +463,14 @@ run_mixed(gray_ctx *c, Render *r, double t_init, double dt_dump, long long n_dum
 	T.prefix = r->d_prefix; /* zeroed at creation: the one render starts at 0 */
 	T.n_renders = 1;
 	T.total = (unsigned long long)r->p.n_rays;
-	CK(launch_mixed_table(T, r->p.n_freq, r->d_queue, r->d_steps, c->stream, c->mixed));
+	if(r->p.spacetime == GRAY_ST_NUMERICAL) {
+		if(!grid_ready(c))
+			return GRAY_ESTATE;
+		CK(launch_dyst_mixed_table(T, c->grid->gp, r->d_queue, r->d_steps, c->stream,
+		                           c->mixed));
+	} else {
+		CK(launch_mixed_table(T, r->p.n_freq, r->d_queue, r->d_steps, c->stream, c->mixed));
+	}
 	return GRAY_OK;
 }
 
@@ -474,14 +481,12 @@ evolve_interval(gray_ctx *c, Render *r, double t, double target, uint64_t n_sub)
 	if(r->p.spacetime == GRAY_ST_NUMERICAL) {
 		if(!grid_ready(c))
 			return GRAY_ESTATE;
-		if(r->desc.precision == GRAY_PREC_FP64)
+		if(r->desc.precision == GRAY_PREC_FP64) {
 			CK(launch_dyst_evolve64(r->p, c->grid->gp, r->d_data, r->d_info, dt,
 			                        (long long)n_sub, r->d_steps, c->stream));
-		else
-			CK(launch_dyst_mixed(r->p, c->grid->gp, r->d_data, r->d_info, t, dt, 1,
-			                     (long long)n_sub, r->d_steps, r->d_queue, c->stream,
-			                     c->mixed));
-		return GRAY_OK;
+			return GRAY_OK;
+		}
+		return run_mixed(c, r, t, dt, 1, (long long)n_sub);
 	}
 	if(r->desc.precision == GRAY_PREC_FP64) {
 		CK(launch_evolve64(r->p, r->d_data, r->d_info, dt, (long long)n_sub,
@@ -518,16 +523,9 @@ evolve_all_impl(gray_ctx *c, Render *r)
 	const gray_render_desc &d = r->desc;
 	int st;
 	if(d.precision == GRAY_PREC_MIXED) {
-		if(r->p.spacetime == GRAY_ST_NUMERICAL)
-			CK(launch_dyst_mixed(r->p, c->grid->gp, r->d_data, r->d_info, d.t_init,
-			                     d.dt_dump, (long long)d.n_dump, (long long)d.n_sub,
-			                     r->d_steps, r->d_queue, c->stream, c->mixed));
-		else {
-			st = run_mixed(c, r, d.t_init, d.dt_dump, (long long)d.n_dump,
-			               (long long)d.n_sub);
-			if(st)
-				return st;
-		}
+		st = run_mixed(c, r, d.t_init, d.dt_dump, (long long)d.n_dump, (long long)d.n_sub);
+		if(st)
+			return st;
 	} else {
 		/* sim-org/gray.c:248-257 */
 		for(uint64_t i = 0; i < d.n_dump;) {
@@ -865,6 +863,25 @@ gray_make_boosted_ks(gray_ctx *c, const gray_grid_desc *gd, double a, double v,
 	CK(launch_boosted_ks(c->grid->gp, c->grid->lvl[level], a, v, axis, t, c->stream));
 	CK(cudaStreamSynchronize(c->stream));
 	c->grid->loaded[level] = true;
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_read_spacetime(gray_ctx *c, int level, float *fields, size_t bytes)
+{
+	if(!c || !fields || (level != 0 && level != 1))
+		return GRAY_EINVAL;
+	if(!c->grid || !c->grid->loaded[level])
+		return GRAY_ESTATE;
+	const gray_grid_desc &gd = c->grid->desc;
+	const size_t npts = (size_t)gd.nx * gd.ny * gd.nz;
+	if(bytes != npts * GRAY_NCOMP * sizeof(float))
+		return GRAY_ESIZE;
+	CK(cudaSetDevice(c->device));
+	CK(cudaMemcpy2DAsync(fields, GRAY_NCOMP * sizeof(float), c->grid->lvl[level],
+	                     GRAY_NSTRIDE * sizeof(float), GRAY_NCOMP * sizeof(float), npts,
+	                     cudaMemcpyDeviceToHost, c->stream));
+	CK(cudaStreamSynchronize(c->stream));
 	return GRAY_OK;
 }
 

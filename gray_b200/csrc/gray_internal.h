@@ -78,14 +78,7 @@ cudaError_t launch_dyst_icond(const RenderParams &p, const GridParams &g, double
 cudaError_t launch_dyst_evolve64(const RenderParams &p, const GridParams &g, double *data,
                                  double *info, double dt, long long n_sub,
                                  unsigned long long *steps, cudaStream_t st);
-cudaError_t launch_dyst_mixed(const RenderParams &p, const GridParams &g, double *data,
-                              double *info, double t_init, double dt_dump,
-                              long long n_dump, long long n_sub,
-                              unsigned long long *steps, unsigned int *queue,
-                              cudaStream_t st, const MixedLaunch &cfg);
 cudaError_t launch_boosted_ks(const GridParams &g, float *lvl, double a, double v,
                               int axis, double t, cudaStream_t st);
-cudaError_t launch_interleave(const float *const *fields_dev, float *lvl, long long npts,
-                              cudaStream_t st);
 
 #endif /* GRAY_INTERNAL_H */

@@ -1,33 +1,342 @@
 /*
- * Numerical-spacetime kernels (interp.cl + dyst.cl).  Filled in by the
- * numerical-spacetime milestone; until then every entry reports
- * cudaErrorNotSupported so the C ABI returns GRAY_ECUDA loudly.
+ * Mixed-precision persistent kernel for numerical spacetimes (interp.cl +
+ * dyst.cl): warp-refilled rays, FP32 gathers of the 40 Christoffel symbols
+ * accumulated with packed f32x2 FMA over component pairs, compensated
+ * (hi, lo) state update, FP64 null-constraint check at the end.
+ *
+ * Grid layout: per time level float [nz][ny][nx][GRAY_NSTRIDE] with the
+ * fields of one grid point contiguous (Gamma 0..39, g 40..49, rho 50, pad),
+ * so the 8 corners of a cell are 8 rows of 208 bytes and the 40 Gamma of a
+ * corner are 10 aligned float4 loads.  The fisheye node coordinates come
+ * from a per-axis table (n + 1 entries) instead of sinh((A i + B)^3) per
+ * field and call (interp.cl:99-121), and the cell search runs once per RHS
+ * for all fields instead of once per field (102 times in the reference).
  */
-#include "gray_internal.h"
+#include <cfloat>
+#include <climits>
 
-cudaError_t
-launch_dyst_icond(const RenderParams &, const GridParams &, double *, double *, cudaStream_t)
+#include "dyst64.cuh"
+#include "mixed_table.h"
+
+namespace {
+
+using dyst64::dyst_getuu64;
+using dyst64::dyst_getdt64;
+
+/* ---------------------------------------------------------------- mixed */
+
+__device__ __forceinline__ float
+rcp_a(float x)
 {
-	return cudaErrorNotSupported;
+	float r;
+	asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+	return r;
 }
 
-cudaError_t
-launch_dyst_evolve64(const RenderParams &, const GridParams &, double *, double *, double,
-                     long long, unsigned long long *, cudaStream_t)
+__device__ __forceinline__ float
+ex2_a(float x)
 {
-	return cudaErrorNotSupported;
+	float r;
+	asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+	return r;
 }
 
-cudaError_t
-launch_dyst_mixed(const RenderParams &, const GridParams &, double *, double *, double, double,
-                  long long, long long, unsigned long long *, unsigned int *, cudaStream_t,
-                  const MixedLaunch &)
+__device__ __forceinline__ float
+lg2_a(float x)
 {
-	return cudaErrorNotSupported;
+	float r;
+	asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+	return r;
 }
 
-cudaError_t
-launch_boosted_ks(const GridParams &, float *, double, double, int, double, cudaStream_t)
+__device__ __forceinline__ float
+sqrt_a(float x)
 {
-	return cudaErrorNotSupported;
+	float r;
+	asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+	return r;
 }
+
+/* cell index of the fisheye map: floor((cbrt(asinh x) - B) / A), with
+ * asinh and cbrt from log2/exp2; only the cell choice depends on it, the
+ * fractional coordinate comes from the exact node table. */
+__device__ __forceinline__ float
+axis_uvw32(const GridParams &g, int a, float x, float Bf, float iAf)
+{
+	const int n = a == 0 ? g.nx : a == 1 ? g.ny : g.nz;
+	float ax = fabsf(x);
+	float as = 0.69314718f * lg2_a(ax + sqrt_a(fmaf(ax, ax, 1.0f)));   /* asinh|x| */
+	float cb = as > 0.0f ? ex2_a(0.33333334f * lg2_a(as)) : 0.0f;       /* cbrt     */
+	cb = copysignf(cb, x);
+	float xi = floorf((cb - Bf) * iAf);
+	int i;
+	if(!(xi >= 0.0f))
+		i = 0;
+	else if(xi > (float)(n - 1))
+		i = n - 1;
+	else
+		i = (int)xi;
+	float x0 = __ldg(g.nodes_f[a] + i);
+	float x1 = __ldg(g.nodes_f[a] + i + 1);
+	float u  = (float)i + (x - x0) * rcp_a(x1 - x0);
+	u = fmaxf(u, 0.0f);
+	return fminf(u, (float)(n - 1));
+}
+
+struct DystConst {
+	float B[3], iA[3];
+};
+
+__device__ __forceinline__ bool
+inside32(const GridParams &g, const float *q)
+{
+#pragma unroll
+	for(int a = 1; a <= 3; ++a)
+		if(!(q[a] >= g.box[a] && q[a] <= g.box[a + 4]))
+			return false;
+	return true;
+}
+
+/* Gamma^mu_ab u^a u^b for mu = t,x,y,z from the 40 interpolated Gamma:
+ * corner rows are gathered as float4 and accumulated in f32x2 pairs. */
+__device__ __forceinline__ void
+dyst_rhs32(const GridParams &g, const DystConst &dc, const float *s, float *ds)
+{
+	const float *u = s + 4;
+	ds[0] = u[0]; ds[1] = u[1]; ds[2] = u[2]; ds[3] = u[3];
+	if(g.physics && !inside32(g, s)) {
+		ds[4] = ds[5] = ds[6] = ds[7] = 0.0f;
+		return;
+	}
+	int i0[3], i1[3];
+	float w[3];
+	const int n[3] = {g.nx, g.ny, g.nz};
+#pragma unroll
+	for(int a = 0; a < 3; ++a) {
+		float uu = axis_uvw32(g, a, s[a + 1], dc.B[a], dc.iA[a]);
+		float fl = floorf(uu);
+		i0[a] = (int)fl;
+		w[a] = uu - fl;
+		i1[a] = min(i0[a] + 1, n[a] - 1);
+	}
+	float ft = 0.0f;
+	if(!g.single) {
+		ft = (s[0] - g.box[0]) * rcp_a(g.box[4] - g.box[0]);
+		if(g.physics)
+			ft = fminf(fmaxf(ft, 0.0f), 1.0f);
+	}
+	float2 acc[20];
+#pragma unroll
+	for(int k = 0; k < 20; ++k)
+		acc[k] = make_float2(0.0f, 0.0f);
+	const float ax = 1.0f - w[0], ay = 1.0f - w[1], az = 1.0f - w[2];
+#pragma unroll
+	for(int c = 0; c < 8; ++c) {
+		float wc = ((c & 1) ? w[0] : ax) * ((c & 2) ? w[1] : ay) * ((c & 4) ? w[2] : az);
+		int ix = (c & 1) ? i1[0] : i0[0];
+		int iy = (c & 2) ? i1[1] : i0[1];
+		int iz = (c & 4) ? i1[2] : i0[2];
+		long long row = (((long long)iz * g.ny + iy) * g.nx + ix) * GRAY_NSTRIDE;
+		const int nl = g.single ? 1 : 2;
+		for(int l = 0; l < nl; ++l) {
+			float wl = g.single ? wc : wc * (l ? ft : 1.0f - ft);
+			const float2 W = make_float2(wl, wl);
+			const float4 *src = (const float4 *)(g.lvl[l] + row);
+#pragma unroll
+			for(int k = 0; k < 10; ++k) {
+				float4 v = __ldg(src + k);
+				acc[2 * k]     = __ffma2_rn(W, make_float2(v.x, v.y), acc[2 * k]);
+				acc[2 * k + 1] = __ffma2_rn(W, make_float2(v.z, v.w), acc[2 * k + 1]);
+			}
+		}
+	}
+	const float *G = (const float *)acc; /* Gamma 0..39 */
+	float p[10];
+	int k = 0;
+#pragma unroll
+	for(int i = 0; i < 4; ++i)
+#pragma unroll
+		for(int j = i; j < 4; ++j) {
+			float uu = u[i] * u[j];
+			p[k++] = i == j ? uu : 2.0f * uu;
+		}
+	float Gm[4];
+#pragma unroll
+	for(int m = 0; m < 4; ++m) {
+		float a = G[10 * m] * p[0];
+#pragma unroll
+		for(int kk = 1; kk < 10; ++kk)
+			a = fmaf(G[10 * m + kk], p[kk], a);
+		Gm[m] = a;
+	}
+#pragma unroll
+	for(int m = 0; m < 4; ++m)
+		ds[4 + m] = fmaf(Gm[0], u[m], -Gm[m]);
+}
+
+__global__ void __launch_bounds__(256, 2)
+dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
+                  unsigned int *__restrict__ queue, unsigned long long *__restrict__ steps)
+{
+	constexpr int ND = 8;
+	const unsigned FULL = 0xffffffffu;
+	const int lane = threadIdx.x & 31;
+	float hi[ND], lo[ND];
+	long long ray = 0;
+	int dump = 0, h = 0, dh_step = 0, n = 0;
+	float dtn = 0.0f;
+	bool active = false, exhausted = false;
+	unsigned long long cnt = 0;
+	const MixedRender *c = nullptr;
+
+	for(;;) {
+		bool need = !active && !exhausted;
+		unsigned mask = __ballot_sync(FULL, need);
+		if(mask) {
+			int leader = __ffs(mask) - 1;
+			unsigned base = 0;
+			if(lane == leader)
+				base = atomicAdd(queue, (unsigned)__popc(mask));
+			base = __shfl_sync(FULL, base, leader);
+			if(need) {
+				unsigned long long gidx = (unsigned long long)base +
+				                          __popc(mask & ((1u << lane) - 1));
+				if(gidx < T.total) {
+					int rr = 0;
+					while(rr + 1 < T.n_renders && T.prefix[rr + 1] <= gidx)
+						++rr;
+					c = &T.renders[rr];
+					ray = (long long)(gidx - T.prefix[rr]);
+					n = (int)((INT_MAX / c->n_sub) * c->n_sub);
+#pragma unroll
+					for(int k = 0; k < ND; ++k) {
+						double v = c->data[k * c->n_rays + ray];
+						hi[k] = (float)v;
+						lo[k] = (float)((double)hi[k] - v);
+					}
+					dump = -1;
+					h = n; /* forces the first dump set-up below */
+					active = true;
+				} else {
+					exhausted = true;
+				}
+			}
+		}
+		if(!__any_sync(FULL, active))
+			break;
+		if(!active)
+			continue;
+		if(h >= n) { /* next dump interval: constants of driver.cl:93 */
+			if(++dump >= c->n_dump) {
+				double s[ND];
+#pragma unroll
+				for(int k = 0; k < ND; ++k) {
+					s[k] = (double)hi[k] - (double)lo[k];
+					c->data[k * c->n_rays + ray] = s[k];
+				}
+				c->info[ray] = dyst_getuu64(g, s);
+				active = false;
+				continue;
+			}
+			double t0 = c->t_init + (double)dump * c->dt_dump;
+			double t1 = c->t_init + (double)(dump + 1) * c->dt_dump;
+			double dt = t1 - t0;
+			dh_step = (int)(dyst_getdt64(dt / (double)c->n_sub) / dt * (double)n);
+			dtn = (float)(dt / (double)n);
+			h = 0;
+			if(dh_step <= 0) { /* zero-length interval: nothing to integrate */
+				h = n;
+				continue;
+			}
+		}
+		int dh = dh_step < n - h ? dh_step : n - h;
+		const float hs = (float)dh * dtn, hh = 0.5f * hs;
+		float k[ND], t[ND], sum[ND];
+		dyst_rhs32(g, dc, hi, k);
+#pragma unroll
+		for(int i = 0; i < ND; ++i) {
+			sum[i] = k[i];
+			t[i] = fmaf(hh, k[i], hi[i]);
+		}
+		dyst_rhs32(g, dc, t, k);
+#pragma unroll
+		for(int i = 0; i < ND; ++i) {
+			sum[i] = fmaf(2.0f, k[i], sum[i]);
+			t[i] = fmaf(hh, k[i], hi[i]);
+		}
+		dyst_rhs32(g, dc, t, k);
+#pragma unroll
+		for(int i = 0; i < ND; ++i) {
+			sum[i] = fmaf(2.0f, k[i], sum[i]);
+			t[i] = fmaf(hs, k[i], hi[i]);
+		}
+		dyst_rhs32(g, dc, t, k);
+		const float h6 = hs * (1.0f / 6.0f);
+		bool bad = false;
+#pragma unroll
+		for(int i = 0; i < ND; ++i) {
+			float inc = h6 * (sum[i] + k[i]);
+			float yv = inc - lo[i];
+			float tv = hi[i] + yv;
+			lo[i] = (tv - hi[i]) - yv;
+			hi[i] = tv;
+			bad |= !(fabsf(tv) <= FLT_MAX);
+		}
+		++cnt;
+		h += dh;
+		if(bad) { /* NaN/Inf (inside the singular region): ray done */
+			double s[ND];
+#pragma unroll
+			for(int kk = 0; kk < ND; ++kk) {
+				s[kk] = (double)hi[kk] - (double)lo[kk];
+				c->data[kk * c->n_rays + ray] = s[kk];
+			}
+			c->info[ray] = s[0] - s[0]; /* NaN marks the ray */
+			active = false;
+		}
+	}
+#pragma unroll
+	for(int o = 16; o > 0; o >>= 1)
+		cnt += __shfl_xor_sync(FULL, cnt, o);
+	if(lane == 0 && cnt)
+		atomicAdd(steps, cnt);
+}
+
+[[maybe_unused]] inline unsigned
+blocks_for(long long n, int block)
+{
+	return (unsigned)((n + block - 1) / block);
+}
+
+} /* namespace */
+
+cudaError_t
+launch_dyst_mixed_table(const MixedTable &T, const GridParams &g, unsigned int *queue,
+                        unsigned long long *steps, cudaStream_t st, const MixedLaunch &cfg)
+{
+	DystConst dc;
+	for(int a = 0; a < 3; ++a) {
+		dc.B[a] = (float)g.B[a];
+		dc.iA[a] = (float)(1.0 / g.A[a]);
+	}
+	cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned int), st);
+	if(e != cudaSuccess)
+		return e;
+	int block = cfg.block > 0 ? cfg.block : 256;
+	int per_sm = cfg.blocks_per_sm;
+	if(per_sm <= 0) {
+		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dyst_mixed_kernel, block, 0);
+		if(e != cudaSuccess)
+			return e;
+		if(per_sm <= 0)
+			per_sm = 1;
+	}
+	long long want = (long long)per_sm * (cfg.sms > 0 ? cfg.sms : 148);
+	long long need = (long long)((T.total + block - 1) / block);
+	unsigned grid = (unsigned)(want < need ? want : need);
+	if(grid == 0)
+		grid = 1;
+	dyst_mixed_kernel<<<grid, block, 0, st>>>(T, g, dc, queue, steps);
+	return cudaGetLastError();
+}
+

@@ -39,4 +39,9 @@ cudaError_t launch_mixed_table(const MixedTable &T, int n_freq, unsigned int *qu
                                unsigned long long *steps, cudaStream_t st,
                                const MixedLaunch &cfg);
 
+/* numerical spacetime: every render of the table on the same grid */
+cudaError_t launch_dyst_mixed_table(const MixedTable &T, const GridParams &g,
+                                    unsigned int *queue, unsigned long long *steps,
+                                    cudaStream_t st, const MixedLaunch &cfg);
+
 #endif /* GRAY_MIXED_TABLE_H */

@@ -192,6 +192,10 @@ int gray_make_boosted_ks(gray_ctx *ctx, const gray_grid_desc *grid, double a,
 /* Swap the two time levels (io.c:279-300 copy_snapshot). */
 int gray_swap_levels(gray_ctx *ctx);
 
+/* Copy one time level back to the host, interleaved [z][y][x][51] floats
+ * (nz*ny*nx*51*4 bytes): inspection of a loaded or generated grid. */
+int gray_read_spacetime(gray_ctx *ctx, int level, float *fields, size_t bytes);
+
 /* ---- allocation-free entry point ----------------------------------- */
 
 /* No counterpart in the reference.  For callers that cannot call

@@ -579,9 +579,13 @@ axis_uvw(double x, double lo, double hi, int n)
 	double B  = cbrt(asinh(lo));
 	double A  = (cbrt(asinh(hi)) - B) / (double)(n - 1);
 	double xi = floor((cbrt(asinh(x)) - B) / A);
-	int i = (int)xi;
-	if(xi < 0.0) i = 0; /* clamp before the int conversion can overflow */
-	if(xi > (double)(n - 1)) i = n - 1;
+	int i; /* clamp before converting (NaN and overflow safe) */
+	if(!(xi >= 0.0))
+		i = 0;
+	else if(xi > (double)(n - 1))
+		i = n - 1;
+	else
+		i = (int)xi;
 	double x0 = node(lo, hi, n, i);
 	double x1 = node(lo, hi, n, i + 1);
 	double u  = (double)i + (x - x0) / (x1 - x0);

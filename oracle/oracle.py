@@ -272,15 +272,17 @@ def boosted_ks_grid(n, lo, hi, t, m=1.0, a=0.7, v=0.3, axis=1, rho=True):
     L = lib()
     q = np.zeros(4)
     buf = np.zeros(50)
-    for k, z in enumerate(xs):
-        for j, y in enumerate(xs):
-            for i, x in enumerate(xs):
-                q[:] = (t, x, y, z)
-                L.orc_boosted_ks(m, a, v, axis, _p(q), _p(buf))
-                out[k, j, i, :50] = buf
-                out[k, j, i, 50] = 1.0 / np.sqrt(x * x + y * y + z * z) if rho else 0.0
-    out = np.nan_to_num(out)
-    return out.astype(np.float32)
+    # the origin node (odd n) gives rho = 1/0 = inf, as tools/generate_data.py does
+    with np.errstate(divide="ignore", over="ignore", invalid="ignore"):
+        for k, z in enumerate(xs):
+            for j, y in enumerate(xs):
+                for i, x in enumerate(xs):
+                    q[:] = (t, x, y, z)
+                    L.orc_boosted_ks(m, a, v, axis, _p(q), _p(buf))
+                    out[k, j, i, :50] = buf
+                    out[k, j, i, 50] = 1.0 / np.sqrt(x * x + y * y + z * z) if rho else 0.0
+        out = np.nan_to_num(out)
+        return out.astype(np.float32)
 
 
 def dyst_rhs(grid, s):
