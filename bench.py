@@ -44,7 +44,8 @@ sys.path.insert(0, ROOT)
 from gray_b200 import configs, flops  # noqa: E402
 
 WORKLOADS = {"torus_rt_1024": configs.TORUS_RT_1024,
-             "kerr_small_64": configs.KERR_SMALL_64}
+             "kerr_small_64": configs.KERR_SMALL_64,
+             "survey_256": None}  # a batch of 256 renders (configs.survey)
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 METRIC = "ray-steps/s"
 
@@ -70,6 +71,10 @@ def parse():
     ap.add_argument("--side", type=int, default=0, help="override the camera side (small runs)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--plan", default="measure", choices=["measure", "estimate", "rpt1", "rpt2"],
+                    help="launch shape of the persistent kernel (measure = autotune)")
+    ap.add_argument("--fp64-renders", type=int, default=16,
+                    help="survey_256: renders run one at a time in FP64 for the comparison")
     return ap.parse_args()
 
 
@@ -218,6 +223,23 @@ def barrier(torch, dist):
     torch.cuda.synchronize()
 
 
+def apply_plan(ctx, api, renders, how):
+    """measure: autotune on these renders (gray_plan); estimate: the rule;
+    rpt1/rpt2: force scalar or packed two-ray kernels."""
+    if how in ("measure", "estimate"):
+        b = ctx.batch(renders)
+        try:
+            p = ctx.plan(b, api.PLAN_MEASURE if how == "measure" else api.PLAN_ESTIMATE)
+        finally:
+            b.close()
+        d = p.as_dict()
+    else:
+        ctx.set_plan(256 if how == "rpt1" else 128, 0, 1 if how == "rpt1" else 2)
+        d = ctx.get_plan().as_dict()
+    d["how"] = how
+    return d
+
+
 def ours_arm(args, cfg, rank, local_rank, world, dist):
     import torch
     from gray_b200 import api
@@ -237,8 +259,9 @@ def ours_arm(args, cfg, rank, local_rank, world, dist):
     peak32 = ctx.measure_peak(api.PREC_MIXED)
     peak64 = ctx.measure_peak(api.PREC_FP64)
 
-    # ---- mixed (headline)
+    # ---- mixed (headline); launch shape from the autotuner (gray_plan)
     rm = ctx.render(dict(cfg, precision=api.PREC_MIXED))
+    plan = apply_plan(ctx, api, [rm], args.plan)
     for _ in range(args.warmup):
         rm.run()
     steps_per_render = rm.steps()
@@ -339,15 +362,145 @@ def ours_arm(args, cfg, rank, local_rank, world, dist):
                    "precision": "mixed", "l2": "flushed (256 MiB write) between steps",
                    "parallelism": "independent renders per GPU" if world > 1 else "single GPU"},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-        "gpu_launches": 2 * args.steps, "clocks": clocks, "fp64": fp64,
+        "gpu_launches": 2 * args.steps, "clocks": clocks, "fp64": fp64, "launch_plan": plan,
         "peaks_measured_tflops": {"fp32": peak32 / 1e12, "fp64": peak64 / 1e12},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def survey_arm(args, rank, local_rank, world, dist):
+    """survey_256: 256 renders (32^2..512^2, random spin / inclination /
+    distance, 4-frequency torus) as ONE batch: one graph-replayed persistent
+    launch per step.  Compared with the FP64 kernel run one render at a time
+    on the first --fp64-renders renders."""
+    import torch
+    from gray_b200 import api
+
+    torch.cuda.set_device(local_rank)
+    ctx = api.Context(local_rank)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    peak32 = ctx.measure_peak(api.PREC_MIXED)
+    cfgs = configs.survey()
+    nf = len(cfgs[0]["nu"])
+    rs = [ctx.render(dict(c, precision=api.PREC_MIXED)) for c in cfgs]
+    n_rays = sum(r.n_rays for r in rs)
+    plan = apply_plan(ctx, api, rs, args.plan)
+    b = ctx.batch(rs)
+    for _ in range(args.warmup):
+        b.run()
+    steps = b.steps()
+    barrier(torch, dist)
+    clk = ClockSampler(local_rank)
+    clk.start()
+    evs = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b.run(wait=False)
+        e1.record()
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    tot = sum(a.elapsed_time(c) for a, c in evs) * 1e-3
+    barrier(torch, dist)
+    tot = max_over_ranks(torch, dist, tot)
+    value = world * steps * args.steps / tot
+    flop_step = flops.mixed_per_step(nf)
+    achieved = steps * flop_step / (tot / args.steps) / 1e12
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak32 / 1e12,
+                "unit": "TFLOP/s", "frac": achieved * 1e12 / peak32, "traffic": None,
+                "peak_source": "FMA-loop microbenchmark in this run",
+                "flop_per_ray_step": flop_step, "kernel": "mixed_kernel<%d> (batched)" % nf}
+
+    # FP64, one render at a time, on a subset; image error of the batched mixed result
+    fp64 = None
+    if not args.no_fp64 and args.fp64_renders > 0:
+        sub = list(range(min(args.fp64_renders, len(cfgs))))
+        r0 = ctx.render(dict(cfgs[0], precision=api.PREC_FP64))
+        r0.run()
+        r0.close()
+        t64, s64, errs = 0.0, 0, []
+        for k in sub:
+            r64 = ctx.render(dict(cfgs[k], precision=api.PREC_FP64))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            flush.zero_()
+            e0.record()
+            r64.run(wait=False)
+            e1.record()
+            torch.cuda.synchronize()
+            t64 += e0.elapsed_time(e1) * 1e-3
+            s64 += r64.steps()
+            d64 = r64.state(api.LAYOUT_SOA)[0]
+            dmx = rs[k].state(api.LAYOUT_SOA)[0]
+            errs.append(max(float(np.linalg.norm(dmx[8 + i] - d64[8 + i]) / np.linalg.norm(d64[8 + i]))
+                            for i in range(nf)))
+            r64.close()
+        v64 = s64 / t64
+        fp64 = {"value": v64, "unit": "ray-steps/s", "renders": len(sub),
+                "mode": "plain FP64 kernel, one render at a time",
+                "mixed_batched_over_fp64_one_at_a_time": value / world / v64,
+                "image_rel_l2_err_max": max(errs), "image_rel_l2_err_median": float(np.median(errs))}
+
+    # end to end: batch + device-to-host copy of every render's state
+    hosts = [torch.empty((r.n_data, r.n_rays), dtype=torch.float64, pin_memory=True).numpy()
+             for r in rs]
+    hinfo = [torch.empty(r.n_rays, dtype=torch.float64, pin_memory=True).numpy() for r in rs]
+    barrier(torch, dist)
+    e2e_t = 0.0
+    for _ in range(args.e2e_steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b.run(wait=False)
+        for r, h, hi in zip(rs, hosts, hinfo):
+            r.state(api.LAYOUT_SOA, out=h, info_out=hi)
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_t += e0.elapsed_time(e1) * 1e-3
+    barrier(torch, dist)
+    e2e_t = max_over_ranks(torch, dist, e2e_t)
+    d2h = sum(h.nbytes for h in hosts) + sum(h.nbytes for h in hinfo)
+    e2e = {"value": world * steps * args.e2e_steps / e2e_t, "unit": "ray-steps/s",
+           "h2d_bytes_per_step": 0, "d2h_bytes_per_step": int(d2h),
+           "note": "render tables are uploaded once at batch creation; replays copy nothing in"}
+    b.close()
+    for r in rs:
+        r.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, cores, rays, secs = cpu_rate(cfgs[len(cfgs) // 2], args.cpu_seconds)
+        cpu = {"value": rate, "unit": "ray-steps/s", "cores": cores, "kind": "port",
+               "sample": "%d rays of survey render %d (stride 7919), every dump interval, %.1f s"
+                         % (rays, len(cfgs) // 2, secs)}
+    ctx.close()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "ray-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64-islands", "data": "synthetic",
+        "config": {"workload": "survey_256", "renders": len(cfgs), "rays_per_step": n_rays,
+                   "seed": configs.SURVEY_SEED, "n_freq": nf, "ray_steps_per_step": steps,
+                   "precision": "mixed", "l2": "flushed (256 MiB write) between steps",
+                   "graph": "one CUDA graph per step (256 icond + 1 persistent kernel)"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": (len(cfgs) + 1) * args.steps, "clocks": clocks, "fp64": fp64,
+        "launch_plan": plan,
     }
     print(json.dumps(line), flush=True)
 
 
 def main():
     args = parse()
-    cfg = dict(WORKLOADS[args.workload])
+    if args.workload == "survey_256":
+        # the reference arm samples the survey's median-index render
+        cfg = configs.survey()[128]
+    else:
+        cfg = dict(WORKLOADS[args.workload])
     if args.side:
         cfg = configs.scaled(cfg, args.side)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -366,7 +519,10 @@ def main():
                              device_id=torch.device("cuda", local_rank))
         dist = D
     try:
-        ours_arm(args, cfg, rank, local_rank, world, dist)
+        if args.workload == "survey_256":
+            survey_arm(args, rank, local_rank, world, dist)
+        else:
+            ours_arm(args, cfg, rank, local_rank, world, dist)
     finally:
         if dist is not None:
             dist.destroy_process_group()

@@ -32,7 +32,10 @@ EXPORTS = [
     "gray_load_spacetime", "gray_load_spacetime_interleaved",
     "gray_make_boosted_ks", "gray_swap_levels", "gray_measure_peak",
     "gray_run_mixed_noalloc", "gray_read_spacetime",
+    "gray_batch_create", "gray_batch_destroy", "gray_batch_run", "gray_batch_steps",
+    "gray_plan", "gray_set_plan", "gray_get_plan",
 ]
+PLAN_ESTIMATE, PLAN_MEASURE = 0, 1
 NOALLOC_MAX_RENDERS = 32
 
 
@@ -58,6 +61,15 @@ class RenderDesc(ctypes.Structure):
         ("torus_hr", ctypes.c_double),
         ("spacetime", ctypes.c_int32), ("precision", ctypes.c_int32),
     ]
+
+
+class LaunchPlan(ctypes.Structure):
+    _fields_ = [("block", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
+                ("rays_per_thread", ctypes.c_int32), ("ns", ctypes.c_double)]
+
+    def as_dict(self):
+        return {"block": self.block, "blocks_per_sm": self.blocks_per_sm,
+                "rays_per_thread": self.rays_per_thread, "trial_ns": self.ns}
 
 
 class GridDesc(ctypes.Structure):
@@ -138,6 +150,13 @@ def lib():
         L.gray_measure_peak.argtypes = [vp, i, P(d)]
         L.gray_run_mixed_noalloc.argtypes = [i, P(RenderDesc), i, P(vp), P(vp), vp, P(u64)]
         L.gray_read_spacetime.argtypes = [vp, i, vp, sz]
+        L.gray_batch_create.argtypes = [vp, P(i), i, P(i)]
+        L.gray_batch_destroy.argtypes = [vp, i]
+        L.gray_batch_run.argtypes = [vp, i, P(d)]
+        L.gray_batch_steps.argtypes = [vp, i, P(u64)]
+        L.gray_plan.argtypes = [vp, i, i, P(LaunchPlan)]
+        L.gray_set_plan.argtypes = [vp, P(LaunchPlan)]
+        L.gray_get_plan.argtypes = [vp, P(LaunchPlan)]
         _lib = L
     return _lib
 
@@ -229,6 +248,35 @@ class Render:
             self.id = 0
 
 
+class Batch:
+    """Many mixed-precision renders in one persistent launch (graph-replayed)."""
+
+    def __init__(self, ctx, renders):
+        self.ctx = ctx
+        self.renders = list(renders)
+        ids = (ctypes.c_int * len(self.renders))(*[r.id for r in self.renders])
+        bid = ctypes.c_int(0)
+        _ck(lib().gray_batch_create(ctx.h, ids, len(self.renders), ctypes.byref(bid)),
+            "gray_batch_create")
+        self.id = bid.value
+
+    def run(self, wait=True):
+        ns = ctypes.c_double(0.0)
+        _ck(lib().gray_batch_run(self.ctx.h, self.id, ctypes.byref(ns) if wait else None),
+            "gray_batch_run")
+        return ns.value
+
+    def steps(self):
+        v = ctypes.c_uint64(0)
+        _ck(lib().gray_batch_steps(self.ctx.h, self.id, ctypes.byref(v)), "gray_batch_steps")
+        return v.value
+
+    def close(self):
+        if self.id:
+            lib().gray_batch_destroy(self.ctx.h, self.id)
+            self.id = 0
+
+
 class Context:
     """One CUDA device; owns every device allocation (gray_create)."""
 
@@ -273,6 +321,23 @@ class Context:
         v = ctypes.c_double(0.0)
         _ck(lib().gray_measure_peak(self.h, precision, ctypes.byref(v)), "gray_measure_peak")
         return v.value
+
+    def batch(self, renders):
+        return Batch(self, renders)
+
+    def plan(self, batch, flags=PLAN_MEASURE):
+        p = LaunchPlan()
+        _ck(lib().gray_plan(self.h, batch.id, flags, ctypes.byref(p)), "gray_plan")
+        return p
+
+    def set_plan(self, block, blocks_per_sm=0, rays_per_thread=2):
+        p = LaunchPlan(block, blocks_per_sm, rays_per_thread, 0.0)
+        _ck(lib().gray_set_plan(self.h, ctypes.byref(p)), "gray_set_plan")
+
+    def get_plan(self):
+        p = LaunchPlan()
+        _ck(lib().gray_get_plan(self.h, ctypes.byref(p)), "gray_get_plan")
+        return p
 
     def read_spacetime(self, grid, level):
         out = np.empty((grid.nz, grid.ny, grid.nx, 51), dtype=np.float32)

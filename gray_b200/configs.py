@@ -26,6 +26,29 @@ TORUS_RT_1024 = dict(
 )
 
 
+SURVEY_SEED = 20261203
+
+
+def survey(n=256, seed=SURVEY_SEED, side_lo=32, side_hi=512):
+    """survey_256: n renders with side log-uniform in [side_lo, side_hi]
+    (pixels log-uniform in 32^2..512^2), spin U[0, 0.998], inclination
+    U[5, 85] deg, camera distance U[100, 1000] M (numpy PCG64, seeded); each
+    uses the torus_rt_1024 torus at 4 frequencies and its step control."""
+    import numpy as np
+    rng = np.random.Generator(np.random.PCG64(seed))
+    side = np.rint(np.exp(rng.uniform(np.log(side_lo), np.log(side_hi), n))).astype(int)
+    a = rng.uniform(0.0, 0.998, n)
+    inc = rng.uniform(5.0, 85.0, n)
+    robs = rng.uniform(100.0, 1000.0, n)
+    out = []
+    for k in range(n):
+        c = dict(TORUS_RT_1024)
+        c.update(a_spin=float(a[k]), i_obs=float(inc[k]), r_obs=float(robs[k]),
+                 n_width=int(side[k]), n_height=int(side[k]))
+        out.append(c)
+    return out
+
+
 def scaled(cfg, side):
     """The same workload on a side x side camera (parity-test sizes)."""
     c = dict(cfg)

@@ -38,6 +38,23 @@ struct Grid {
 	GridParams gp;
 };
 
+struct Batch {
+	std::vector<int> ids;
+	int spacetime = GRAY_ST_KERR;
+	int n_freq = 0;
+	unsigned long long total = 0;
+	void *block = nullptr;          /* table | prefix | queue | steps      */
+	size_t bytes = 0;
+	MixedRender *d_table = nullptr;
+	unsigned long long *d_prefix = nullptr;
+	unsigned int *d_queue = nullptr;
+	unsigned long long *d_steps = nullptr;
+	std::vector<MixedRender> host_table;
+	cudaGraphExec_t exec = nullptr;
+	MixedLaunch graph_cfg = {0, 0, 0, 0};
+	cudaStream_t graph_stream = nullptr;
+};
+
 struct gray_ctx {
 	int device = 0;
 	size_t budget = 0;
@@ -50,7 +67,12 @@ struct gray_ctx {
 	int next_id = 1;
 	Grid *grid = nullptr;
 	int evolve64_block = 128;
-	MixedLaunch mixed = {256, 0, 0};
+	/* default plan (GRAY_PLAN_ESTIMATE): one ray per thread, 256-thread
+	 * blocks -- the shape the measuring planner picks on B200 for the
+	 * analytic torus renders */
+	MixedLaunch mixed = {256, 0, 0, 1};
+	std::map<int, Batch *> batches;
+	int next_batch = 1;
 };
 
 namespace {
@@ -333,6 +355,14 @@ gray_destroy(gray_ctx *c)
 	cudaSetDevice(c->device);
 	if(c->stream)
 		cudaStreamSynchronize(c->stream);
+	for(auto &kv : c->batches) {
+		Batch *b = kv.second;
+		if(b->exec)
+			cudaGraphExecDestroy(b->exec);
+		dfree(c, b->block, b->bytes);
+		delete b;
+	}
+	c->batches.clear();
 	for(auto &kv : c->renders) {
 		Render *r = kv.second;
 		dfree(c, r->d_data, r->bytes);
@@ -415,6 +445,10 @@ gray_render_destroy(gray_ctx *c, int id)
 	Render *r = find(c, id);
 	if(!r)
 		return GRAY_ENOTFOUND;
+	for(auto &kv : c->batches)
+		for(int bid : kv.second->ids)
+			if(bid == id)
+				return GRAY_ESTATE; /* still part of a batch */
 	CK(cudaSetDevice(c->device));
 	CK(cudaStreamSynchronize(c->stream));
 	dfree(c, r->d_data, r->bytes);
@@ -911,5 +945,320 @@ gray_swap_levels(gray_ctx *c)
 	g->loaded[1] = b;
 	g->gp.lvl[0] = g->lvl[0];
 	g->gp.lvl[1] = g->lvl[1];
+	return GRAY_OK;
+}
+
+/* ---- batches, plans, graphs ---------------------------------------- */
+
+static Batch *
+find_batch(gray_ctx *c, int id)
+{
+	if(!c)
+		return nullptr;
+	auto it = c->batches.find(id);
+	return it == c->batches.end() ? nullptr : it->second;
+}
+
+static void
+drop_graph(Batch *b)
+{
+	if(b->exec) {
+		cudaGraphExecDestroy(b->exec);
+		b->exec = nullptr;
+	}
+}
+
+extern "C" int
+gray_batch_create(gray_ctx *c, const int *ids, int n, int *batch_id)
+{
+	if(!c || !ids || n < 1 || !batch_id)
+		return GRAY_EINVAL;
+	Batch *b = new(std::nothrow) Batch;
+	if(!b)
+		return GRAY_ENOMEM;
+	b->host_table.resize(n);
+	std::vector<unsigned long long> prefix(n);
+	for(int i = 0; i < n; ++i) {
+		Render *r = find(c, ids[i]);
+		if(!r) {
+			delete b;
+			return GRAY_ENOTFOUND;
+		}
+		for(int j = 0; j < i; ++j)
+			if(ids[j] == ids[i]) {
+				delete b;
+				return GRAY_EINVAL; /* a render appears twice */
+			}
+		const gray_render_desc &d = r->desc;
+		if(d.precision != GRAY_PREC_MIXED ||
+		   (i > 0 && (d.spacetime != b->spacetime || d.n_freq != b->n_freq))) {
+			delete b;
+			return GRAY_EINVAL;
+		}
+		b->spacetime = d.spacetime;
+		b->n_freq = d.n_freq;
+		memset(&b->host_table[i], 0, sizeof(MixedRender));
+		fill_mixed_render(r->p, r->d_data, r->d_info, d.t_init, d.dt_dump,
+		                  (long long)d.n_dump, (long long)d.n_sub, &b->host_table[i]);
+		prefix[i] = b->total;
+		b->total += (unsigned long long)r->p.n_rays;
+		b->ids.push_back(ids[i]);
+	}
+	if(b->total > (1ull << 31)) {
+		delete b;
+		return GRAY_EINVAL; /* the ray queue is a 32-bit counter */
+	}
+	CK(cudaSetDevice(c->device));
+	const size_t tab = ((size_t)n * sizeof(MixedRender) + 255) / 256 * 256;
+	const size_t pre = ((size_t)n * sizeof(unsigned long long) + 255) / 256 * 256;
+	b->bytes = tab + pre + 256;
+	int st = dalloc(c, &b->block, b->bytes);
+	if(st) {
+		delete b;
+		return st;
+	}
+	b->d_table = (MixedRender *)b->block;
+	b->d_prefix = (unsigned long long *)((char *)b->block + tab);
+	b->d_queue = (unsigned int *)((char *)b->block + tab + pre);
+	b->d_steps = (unsigned long long *)((char *)b->block + tab + pre + 128);
+	cudaError_t e = cudaMemcpyAsync(b->d_table, b->host_table.data(),
+	                                (size_t)n * sizeof(MixedRender), cudaMemcpyHostToDevice,
+	                                c->stream);
+	if(e == cudaSuccess)
+		e = cudaMemcpyAsync(b->d_prefix, prefix.data(), (size_t)n * sizeof(unsigned long long),
+		                    cudaMemcpyHostToDevice, c->stream);
+	if(e == cudaSuccess)
+		e = cudaMemsetAsync((char *)b->block + tab + pre, 0, 256, c->stream);
+	if(e == cudaSuccess)
+		e = cudaStreamSynchronize(c->stream);
+	if(e != cudaSuccess) {
+		dfree(c, b->block, b->bytes);
+		delete b;
+		return from_cuda(e);
+	}
+	*batch_id = c->next_batch++;
+	c->batches[*batch_id] = b;
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_batch_destroy(gray_ctx *c, int id)
+{
+	Batch *b = find_batch(c, id);
+	if(!b)
+		return GRAY_ENOTFOUND;
+	CK(cudaSetDevice(c->device));
+	CK(cudaStreamSynchronize(c->stream));
+	drop_graph(b);
+	dfree(c, b->block, b->bytes);
+	c->batches.erase(id);
+	delete b;
+	return GRAY_OK;
+}
+
+/* Enqueue the batch: initial conditions of every render, counters reset,
+ * one persistent launch over the whole table. */
+static int
+batch_enqueue(gray_ctx *c, Batch *b, const MixedLaunch &cfg, const MixedTable &T)
+{
+	for(int id : b->ids) {
+		Render *r = find(c, id);
+		if(r->p.spacetime == GRAY_ST_NUMERICAL)
+			CK(launch_dyst_icond(r->p, c->grid->gp, r->d_data, r->d_info, c->stream));
+		else
+			CK(launch_icond64(r->p, r->d_data, r->d_info, c->stream));
+	}
+	CK(cudaMemsetAsync(b->d_steps, 0, sizeof(unsigned long long), c->stream));
+	if(b->spacetime == GRAY_ST_NUMERICAL)
+		CK(launch_dyst_mixed_table(T, c->grid->gp, b->d_queue, b->d_steps, c->stream, cfg));
+	else
+		CK(launch_mixed_table(T, b->n_freq, b->d_queue, b->d_steps, c->stream, cfg));
+	return GRAY_OK;
+}
+
+static MixedTable
+batch_table(const Batch *b)
+{
+	MixedTable T;
+	T.renders = b->d_table;
+	T.prefix = b->d_prefix;
+	T.n_renders = (int)b->ids.size();
+	T.total = b->total;
+	return T;
+}
+
+static bool
+same_cfg(const MixedLaunch &a, const MixedLaunch &b)
+{
+	return a.block == b.block && a.blocks_per_sm == b.blocks_per_sm && a.sms == b.sms &&
+	       a.rays_per_thread == b.rays_per_thread;
+}
+
+extern "C" int
+gray_batch_run(gray_ctx *c, int id, double *ns)
+{
+	Batch *b = find_batch(c, id);
+	if(!b)
+		return GRAY_ENOTFOUND;
+	if(b->spacetime == GRAY_ST_NUMERICAL && !grid_ready(c))
+		return GRAY_ESTATE;
+	CK(cudaSetDevice(c->device));
+	if(b->exec && (!same_cfg(b->graph_cfg, c->mixed) || b->graph_stream != c->stream))
+		drop_graph(b);
+	if(!b->exec) {
+		/* capture once; the graph is replayed by every later run */
+		cudaGraph_t g = nullptr;
+		CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+		int st = batch_enqueue(c, b, c->mixed, batch_table(b));
+		cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+		if(st) {
+			if(g)
+				cudaGraphDestroy(g);
+			return st;
+		}
+		if(e != cudaSuccess)
+			return from_cuda(e);
+		e = cudaGraphInstantiate(&b->exec, g, 0);
+		cudaGraphDestroy(g);
+		if(e != cudaSuccess) {
+			b->exec = nullptr;
+			return from_cuda(e);
+		}
+		b->graph_cfg = c->mixed;
+		b->graph_stream = c->stream;
+	}
+	int st = timed_begin(c);
+	if(st)
+		return st;
+	CK(cudaGraphLaunch(b->exec, c->stream));
+	for(int rid : b->ids)
+		find(c, rid)->has_state = true;
+	return timed_end(c, ns);
+}
+
+extern "C" int
+gray_batch_steps(gray_ctx *c, int id, uint64_t *steps)
+{
+	Batch *b = find_batch(c, id);
+	if(!b)
+		return GRAY_ENOTFOUND;
+	if(!steps)
+		return GRAY_EINVAL;
+	CK(cudaSetDevice(c->device));
+	unsigned long long v = 0;
+	CK(cudaMemcpyAsync(&v, b->d_steps, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
+	CK(cudaStreamSynchronize(c->stream));
+	*steps = v;
+	return GRAY_OK;
+}
+
+static int
+check_plan(const gray_launch_plan *p)
+{
+	if(!p || (p->rays_per_thread != 1 && p->rays_per_thread != 2))
+		return GRAY_EINVAL;
+	const int maxb = p->rays_per_thread == 2 ? 128 : 256;
+	if(p->block < 32 || p->block > maxb || p->block % 32 || p->blocks_per_sm < 0)
+		return GRAY_EINVAL;
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_set_plan(gray_ctx *c, const gray_launch_plan *p)
+{
+	if(!c)
+		return GRAY_EINVAL;
+	int st = check_plan(p);
+	if(st)
+		return st;
+	c->mixed.block = p->block;
+	c->mixed.blocks_per_sm = p->blocks_per_sm;
+	c->mixed.rays_per_thread = p->rays_per_thread;
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_get_plan(const gray_ctx *c, gray_launch_plan *p)
+{
+	if(!c || !p)
+		return GRAY_EINVAL;
+	p->block = c->mixed.block;
+	p->blocks_per_sm = c->mixed.blocks_per_sm;
+	p->rays_per_thread = c->mixed.rays_per_thread;
+	p->ns = 0.0;
+	return GRAY_OK;
+}
+
+/* Candidates: rays per thread {2, 1} x block {64, 128(, 256)} x blocks per
+ * SM {all that fit, half of them}.  Each is timed (best of two) over the
+ * first two dump intervals of every render in the batch, launched directly
+ * (not through the graph). */
+extern "C" int
+gray_plan(gray_ctx *c, int id, int flags, gray_launch_plan *best)
+{
+	Batch *b = find_batch(c, id);
+	if(!b)
+		return GRAY_ENOTFOUND;
+	if(!best || (flags != GRAY_PLAN_ESTIMATE && flags != GRAY_PLAN_MEASURE))
+		return GRAY_EINVAL;
+	CK(cudaSetDevice(c->device));
+	if(flags == GRAY_PLAN_ESTIMATE || b->spacetime == GRAY_ST_NUMERICAL) {
+		/* the rule: 256 threads, one ray each (the numerical kernel has
+		 * only this shape) */
+		c->mixed = MixedLaunch{256, 0, c->sms, 1};
+		return gray_get_plan(c, best);
+	}
+	/* trial table: the first two dump intervals of every render */
+	std::vector<MixedRender> trial = b->host_table;
+	for(auto &m : trial)
+		m.dump_end = m.dump_begin + (m.dump_end - m.dump_begin > 2 ? 2 : m.dump_end - m.dump_begin);
+	CK(cudaMemcpyAsync(b->d_table, trial.data(), trial.size() * sizeof(MixedRender),
+	                   cudaMemcpyHostToDevice, c->stream));
+	MixedTable T = batch_table(b);
+	MixedLaunch cand[16];
+	int nc = 0;
+	for(int rpt = 2; rpt >= 1; --rpt)
+		for(int blk = 64; blk <= (rpt == 2 ? 128 : 256); blk *= 2) {
+			MixedLaunch m = {blk, 0, c->sms, rpt};
+			int occ = 0;
+			if(mixed_occupancy(b->n_freq, m, &occ) != cudaSuccess || occ <= 0)
+				continue;
+			cand[nc++] = m;
+			if(occ >= 2) {
+				m.blocks_per_sm = occ / 2;
+				cand[nc++] = m;
+			}
+		}
+	double best_ns = 1e300;
+	MixedLaunch best_cfg = c->mixed;
+	int st = GRAY_OK;
+	for(int k = 0; k < nc && !st; ++k) {
+		for(int rep = 0; rep < 2 && !st; ++rep) {
+			double ns = 0.0;
+			if((st = timed_begin(c)))
+				break;
+			if((st = batch_enqueue(c, b, cand[k], T)))
+				break;
+			if((st = timed_end(c, &ns)))
+				break;
+			if(ns < best_ns) {
+				best_ns = ns;
+				best_cfg = cand[k];
+			}
+		}
+	}
+	/* restore the full schedule */
+	cudaError_t e = cudaMemcpyAsync(b->d_table, b->host_table.data(),
+	                                b->host_table.size() * sizeof(MixedRender),
+	                                cudaMemcpyHostToDevice, c->stream);
+	if(e == cudaSuccess)
+		e = cudaStreamSynchronize(c->stream);
+	if(st)
+		return st;
+	if(e != cudaSuccess)
+		return from_cuda(e);
+	c->mixed = best_cfg;
+	gray_get_plan(c, best);
+	best->ns = best_ns;
 	return GRAY_OK;
 }

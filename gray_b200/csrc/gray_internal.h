@@ -70,6 +70,7 @@ struct MixedLaunch {
 	int block;        /* threads per block                              */
 	int blocks_per_sm;/* 0: from the occupancy calculator               */
 	int sms;
+	int rays_per_thread; /* 1 or 2 (analytic kernel only)               */
 };
 
 /* numerical spacetime */

@@ -214,7 +214,7 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 						hi[k] = (float)v;
 						lo[k] = (float)((double)hi[k] - v);
 					}
-					dump = -1;
+					dump = c->dump_begin - 1;
 					h = n; /* forces the first dump set-up below */
 					active = true;
 				} else {
@@ -227,7 +227,7 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 		if(!active)
 			continue;
 		if(h >= n) { /* next dump interval: constants of driver.cl:93 */
-			if(++dump >= c->n_dump) {
+			if(++dump >= c->dump_end) {
 				double s[ND];
 #pragma unroll
 				for(int k = 0; k < ND; ++k) {

@@ -1,23 +1,27 @@
 /*
  * Mixed-precision persistent geodesic kernel (analytic Kerr-Schild + torus
- * transfer).  One launch integrates every dump interval of every ray of
- * one or many renders:
+ * transfer).  One launch integrates a window of dump intervals of every ray
+ * of one or many renders:
  *
  *  - persistent warps pull rays from a global queue; a warp ballot finds the
- *    lanes whose ray terminated (horizon capture, or all dumps done) and
- *    refills exactly those lanes, so captured rays do not idle SIMD lanes
- *    while their neighbours keep integrating;
+ *    lanes whose ray terminated (horizon capture, or its dump window done)
+ *    and refills exactly those lanes, so captured rays do not idle SIMD
+ *    lanes while their neighbours keep integrating;
  *  - the RHS (KS.cl:263-378), RK4 stages (RK4.cl:37-47) and transfer
- *    (rt.cl:185-198 form with the analytic torus) run in FP32, using the
- *    approximate rcp/rsqrt/ex2/lg2 instructions instead of IEEE divide and
- *    square-root sequences;
- *  - FP64 is kept where it matters: the state update is compensated (Kahan:
+ *    (rt.cl:185-198 form with the analytic torus) run in FP32 with the
+ *    approximate rcp/rsqrt/ex2/lg2 instructions in place of IEEE divide and
+ *    square-root sequences; with two rays per thread the whole step runs in
+ *    sm_100 packed f32x2 arithmetic (one FFMA2/FMUL2/FADD2 issue slot serves
+ *    both rays);
+ *  - FP64 is kept where it matters: the state update is compensated (Kahan
  *    hi + lo pairs of FP32), the Kerr-Schild radius root (KS.cl:48-55) is
  *    evaluated in FP64 near the horizon where the stop rule and step-size
  *    rule (phys.cl:48-64) read it, and the null-constraint diagnostic
  *    (KS.cl:164-168) is computed in FP64 from the final state;
  *  - the integer-tick substep loop of driver.cl:81-99 is kept, so dump
- *    boundaries are hit exactly as in the FP64 kernel.
+ *    boundaries are hit exactly as in the FP64 kernel;
+ *  - each ray's render constants live in registers (loaded when the ray is
+ *    loaded), not re-read from the table every RHS.
  */
 #include <climits>
 
@@ -25,6 +29,8 @@
 #include "mixed_table.h"
 
 namespace {
+
+/* ---------------------------------------------------------- scalar MUFU */
 
 __device__ __forceinline__ float
 rcp_a(float x)
@@ -66,175 +72,262 @@ lg2_a(float x)
 	return r;
 }
 
-struct Aux32 {
-	float r, ir, f, lx, ly, lz, flu, iss;
+/* ------------------------------------------- lane types: float and f32x2 */
+
+struct F2 {
+	float2 v;
+};
+struct M2 {
+	bool x, y;
 };
 
-/* KS.cl:263-378 in FP32: the same Chan et al. grouping, with the five
- * divides and two square roots folded into 2 rsqrt + 2 rcp. */
-__device__ __forceinline__ void
-ks_rhs32(const MixedRender &c, const float *s, float *ds, Aux32 &aux)
-{
-	const float a = c.a, aa = c.aa;
-	const float x = s[1], y = s[2], z = s[3];
-	const float ut = s[4], ux = s[5], uy = s[6], uz = s[7];
+__device__ __forceinline__ F2 mk2(float a, float b) { F2 r; r.v = make_float2(a, b); return r; }
 
-	float f, dx_f, dy_f, dz_f;
-	float lx, dx_lx, dy_lx, dz_lx;
-	float ly, dx_ly, dy_ly, dz_ly;
-	float lz, dx_lz, dy_lz, dz_lz;
-	float dx_r, dy_r, dz_r, r, ir, iss, tmp;
+template <typename V> __device__ __forceinline__ V bc(float c);
+template <> __device__ __forceinline__ float bc<float>(float c) { return c; }
+template <> __device__ __forceinline__ F2 bc<F2>(float c) { return mk2(c, c); }
+
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { F2 r; r.v = __fadd2_rn(a.v, b.v); return r; }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { F2 r; r.v = __fmul2_rn(a.v, b.v); return r; }
+__device__ __forceinline__ F2 operator-(F2 a, F2 b)
+{
+	F2 r;
+	r.v = __ffma2_rn(b.v, make_float2(-1.0f, -1.0f), a.v);
+	return r;
+}
+__device__ __forceinline__ F2 operator-(F2 a) { F2 r; r.v = __fmul2_rn(a.v, make_float2(-1.0f, -1.0f)); return r; }
+
+__device__ __forceinline__ float fmav(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ F2 fmav(F2 a, F2 b, F2 c) { F2 r; r.v = __ffma2_rn(a.v, b.v, c.v); return r; }
+
+#define LANEWISE(name, f)                                                       \
+	__device__ __forceinline__ float name(float a) { return f(a); }             \
+	__device__ __forceinline__ F2 name(F2 a) { return mk2(f(a.v.x), f(a.v.y)); }
+LANEWISE(rcpv, rcp_a)
+LANEWISE(rsqv, rsqrt_a)
+LANEWISE(ex2v, ex2_a)
+LANEWISE(lg2v, lg2_a)
+#undef LANEWISE
+
+__device__ __forceinline__ bool gtv(float a, float b) { return a > b; }
+__device__ __forceinline__ M2 gtv(F2 a, F2 b) { M2 m = {a.v.x > b.v.x, a.v.y > b.v.y}; return m; }
+__device__ __forceinline__ bool andv(bool a, bool b) { return a && b; }
+__device__ __forceinline__ M2 andv(M2 a, M2 b) { M2 m = {a.x && b.x, a.y && b.y}; return m; }
+__device__ __forceinline__ float selv(bool m, float a, float b) { return m ? a : b; }
+__device__ __forceinline__ F2 selv(M2 m, F2 a, F2 b) { return mk2(m.x ? a.v.x : b.v.x, m.y ? a.v.y : b.v.y); }
+
+template <typename V> struct MaskOf;
+template <> struct MaskOf<float> { typedef bool T; };
+template <> struct MaskOf<F2> { typedef M2 T; };
+
+/* lane k of a V (k is a compile-time constant after unrolling) */
+__device__ __forceinline__ float getl(float a, int) { return a; }
+__device__ __forceinline__ float getl(F2 a, int k) { return k ? a.v.y : a.v.x; }
+__device__ __forceinline__ void setl(float &a, int, float x) { a = x; }
+__device__ __forceinline__ void setl(F2 &a, int k, float x)
+{
+	if(k)
+		a.v.y = x;
+	else
+		a.v.x = x;
+}
+
+template <typename V> struct Lanes;
+template <> struct Lanes<float> { static constexpr int N = 1; };
+template <> struct Lanes<F2> { static constexpr int N = 2; };
+
+/* ------------------------------------------------ per-ray render constants */
+
+template <typename V, int NF>
+struct RC {
+	V a, aa, risco, kappa, n0_rp15, ihr2, torus;
+	V nupow[NF > 0 ? NF : 1], nuinv2[NF > 0 ? NF : 1];
+};
+
+template <typename V, int NF>
+__device__ __forceinline__ void
+load_rc(RC<V, NF> &rc, int k, const MixedRender &c)
+{
+	setl(rc.a, k, c.a);
+	setl(rc.aa, k, c.aa);
+	setl(rc.risco, k, c.risco);
+	setl(rc.kappa, k, c.kappa);
+	setl(rc.n0_rp15, k, c.n0_rp15);
+	setl(rc.ihr2, k, c.ihr2_log2e);
+	setl(rc.torus, k, c.flow == GRAY_FLOW_TORUS ? 1.0f : 0.0f);
+#pragma unroll
+	for(int i = 0; i < NF; ++i) {
+		setl(rc.nupow[i], k, c.nupow[i]);
+		setl(rc.nuinv2[i], k, c.nuinv2[i]);
+	}
+}
+
+/* -------------------------------------------------------------- the RHS */
+
+template <typename V>
+struct Aux {
+	V r, ir, f, lx, ly, lz, flu, iss;
+};
+
+/* KS.cl:263-378 in FP32: the Chan et al. grouping, with the five divides
+ * and two square roots folded into 2 rsqrt + 2 rcp. */
+template <typename V, int NF>
+__device__ __forceinline__ void
+ks_rhs(const RC<V, NF> &c, const V *s, V *ds, Aux<V> &aux)
+{
+	const V a = c.a, aa = c.aa;
+	const V x = s[1], y = s[2], z = s[3];
+	const V ut = s[4], ux = s[5], uy = s[6], uz = s[7];
+	const V half = bc<V>(0.5f), one = bc<V>(1.0f), two = bc<V>(2.0f);
+
+	V f, dx_f, dy_f, dz_f;
+	V lx, dx_lx, dy_lx, dz_lx;
+	V ly, dx_ly, dy_ly, dz_ly;
+	V lz, dx_lz, dy_lz, dz_lz;
+	V dx_r, dy_r, dz_r, r, ir, iss, tmp;
 	{
-		float zz  = z * z;
-		float kk  = 0.5f * (fmaf(x, x, fmaf(y, y, zz)) - aa);
-		float d2  = fmaf(kk, kk, aa * zz);
-		float idd = rsqrt_a(d2);
-		float dd  = d2 * idd;
-		float rr  = dd + kk;
-		ir  = rsqrt_a(rr);
+		V zz  = z * z;
+		V azz = aa * zz;
+		V kk  = half * (fmav(x, x, fmav(y, y, zz)) - aa);
+		V d2  = fmav(kk, kk, azz);
+		V idd = rsqv(d2);
+		V dd  = d2 * idd;
+		V rr  = dd + kk;
+		ir  = rsqv(rr);
 		r   = rr * ir;
-		float ss = rr + aa;
-		iss  = rcp_a(ss);
-		tmp  = 0.5f * ir * idd;
-		dz_r = tmp * ss * z;
+		V ss = rr + aa;
+		iss  = rcpv(ss);
+		tmp  = half * (ir * idd);
+		dz_r = (tmp * ss) * z;
 		tmp  = tmp * rr;
 		dy_r = tmp * y;
 		dx_r = tmp * x;
-		tmp  = 2.0f * rr * rcp_a(fmaf(rr, rr, aa * zz));
-		float tmp2 = fmaf(-2.0f * rr, tmp, 3.0f);
+		tmp  = (two * rr) * rcpv(fmav(rr, rr, azz));
+		V tmp2 = fmav(-(two * rr), tmp, bc<V>(3.0f));
 		f    = tmp * r;
-		dx_f = tmp * dx_r * tmp2;
-		dy_f = tmp * dy_r * tmp2;
-		dz_f = tmp * fmaf(dz_r, tmp2, -(tmp * aa * z * ir));
+		V tt2 = tmp * tmp2;
+		dx_f = tt2 * dx_r;
+		dy_f = tt2 * dy_r;
+		dz_f = fmav(tt2, dz_r, -((tmp * tmp) * (aa * (z * ir))));
 	}
 	{
-		float m2r  = -2.0f * r;
-		float issr = iss * r;
-		float issa = iss * a;
+		V m2r  = -(two * r);
+		V issr = iss * r;
+		V issa = iss * a;
 
-		lx    = iss * fmaf(x, r, y * a);
-		tmp   = iss * fmaf(m2r, lx, x);
-		dx_lx = fmaf(tmp, dx_r, issr);
-		dy_lx = fmaf(tmp, dy_r, issa);
+		lx    = iss * fmav(x, r, y * a);
+		tmp   = iss * fmav(m2r, lx, x);
+		dx_lx = fmav(tmp, dx_r, issr);
+		dy_lx = fmav(tmp, dy_r, issa);
 		dz_lx = tmp * dz_r;
 
-		ly    = iss * fmaf(y, r, -(x * a));
-		tmp   = iss * fmaf(m2r, ly, y);
-		dx_ly = fmaf(tmp, dx_r, -issa);
-		dy_ly = fmaf(tmp, dy_r, issr);
+		ly    = iss * fmav(y, r, -(x * a));
+		tmp   = iss * fmav(m2r, ly, y);
+		dx_ly = fmav(tmp, dx_r, -issa);
+		dy_ly = fmav(tmp, dy_r, issr);
 		dz_ly = tmp * dz_r;
 
 		lz    = z * ir;
-		tmp   = -lz * ir;
+		tmp   = -(lz * ir);
 		dx_lz = tmp * dx_r;
 		dy_lz = tmp * dy_r;
-		dz_lz = fmaf(tmp, dz_r, ir);
+		dz_lz = fmav(tmp, dz_r, ir);
 	}
-	float lu  = fmaf(lz, uz, fmaf(ly, uy, fmaf(lx, ux, ut)));
-	float flu = f * lu;
-	float Dx0 = fmaf(dx_f, lu, f * fmaf(dx_lz, uz, fmaf(dx_ly, uy, dx_lx * ux)));
-	float Dy0 = fmaf(dy_f, lu, f * fmaf(dy_lz, uz, fmaf(dy_ly, uy, dy_lx * ux)));
-	float Dz0 = fmaf(dz_f, lu, f * fmaf(dz_lz, uz, fmaf(dz_ly, uy, dz_lx * ux)));
+	V lu  = fmav(lz, uz, fmav(ly, uy, fmav(lx, ux, ut)));
+	V flu = f * lu;
+	V Dx0 = fmav(dx_f, lu, f * fmav(dx_lz, uz, fmav(dx_ly, uy, dx_lx * ux)));
+	V Dy0 = fmav(dy_f, lu, f * fmav(dy_lz, uz, fmav(dy_ly, uy, dy_lx * ux)));
+	V Dz0 = fmav(dz_f, lu, f * fmav(dz_lz, uz, fmav(dz_ly, uy, dz_lx * ux)));
 
-	float Dx1 = fmaf(Dx0, lx, flu * dx_lx);
-	float Dx2 = fmaf(Dx0, ly, flu * dx_ly);
-	float Dx3 = fmaf(Dx0, lz, flu * dx_lz);
-	float Dy1 = fmaf(Dy0, lx, flu * dy_lx);
-	float Dy2 = fmaf(Dy0, ly, flu * dy_ly);
-	float Dy3 = fmaf(Dy0, lz, flu * dy_lz);
-	float Dz1 = fmaf(Dz0, lx, flu * dz_lx);
-	float Dz2 = fmaf(Dz0, ly, flu * dz_ly);
-	float Dz3 = fmaf(Dz0, lz, flu * dz_lz);
+	V Dx1 = fmav(Dx0, lx, flu * dx_lx);
+	V Dx2 = fmav(Dx0, ly, flu * dx_ly);
+	V Dx3 = fmav(Dx0, lz, flu * dx_lz);
+	V Dy1 = fmav(Dy0, lx, flu * dy_lx);
+	V Dy2 = fmav(Dy0, ly, flu * dy_ly);
+	V Dy3 = fmav(Dy0, lz, flu * dy_lz);
+	V Dz1 = fmav(Dz0, lx, flu * dz_lx);
+	V Dz2 = fmav(Dz0, ly, flu * dz_ly);
+	V Dz3 = fmav(Dz0, lz, flu * dz_lz);
 
-	float hDxu = 0.5f * fmaf(Dx3, uz, fmaf(Dx2, uy, fmaf(Dx1, ux, Dx0 * ut)));
-	float hDyu = 0.5f * fmaf(Dy3, uz, fmaf(Dy2, uy, fmaf(Dy1, ux, Dy0 * ut)));
-	float hDzu = 0.5f * fmaf(Dz3, uz, fmaf(Dz2, uy, fmaf(Dz1, ux, Dz0 * ut)));
+	V hDxu = half * fmav(Dx3, uz, fmav(Dx2, uy, fmav(Dx1, ux, Dx0 * ut)));
+	V hDyu = half * fmav(Dy3, uz, fmav(Dy2, uy, fmav(Dy1, ux, Dy0 * ut)));
+	V hDzu = half * fmav(Dz3, uz, fmav(Dz2, uy, fmav(Dz1, ux, Dz0 * ut)));
 
-	float uD0 = fmaf(uz, Dz0, fmaf(uy, Dy0, ux * Dx0));
-	float uD1 = fmaf(uz, Dz1, fmaf(uy, Dy1, ux * Dx1));
-	float uD2 = fmaf(uz, Dz2, fmaf(uy, Dy2, ux * Dx2));
-	float uD3 = fmaf(uz, Dz3, fmaf(uy, Dy3, ux * Dx3));
+	V uD0 = fmav(uz, Dz0, fmav(uy, Dy0, ux * Dx0));
+	V uD1 = fmav(uz, Dz1, fmav(uy, Dy1, ux * Dx1));
+	V uD2 = fmav(uz, Dz2, fmav(uy, Dy2, ux * Dx2));
+	V uD3 = fmav(uz, Dz3, fmav(uy, Dy3, ux * Dx3));
 
-	tmp = f * fmaf(lz, uD3 - hDzu, fmaf(ly, uD2 - hDyu, fmaf(lx, uD1 - hDxu, -uD0)));
+	tmp = f * fmav(lz, uD3 - hDzu, fmav(ly, uD2 - hDyu, fmav(lx, uD1 - hDxu, -uD0)));
 
 	ds[0] = ut;
 	ds[1] = ux;
 	ds[2] = uy;
 	ds[3] = uz;
 	ds[4] = uD0 - tmp;
-	ds[5] = fmaf(lx, tmp, hDxu - uD1);
-	ds[6] = fmaf(ly, tmp, hDyu - uD2);
-	ds[7] = fmaf(lz, tmp, hDzu - uD3);
+	ds[5] = fmav(lx, tmp, hDxu - uD1);
+	ds[6] = fmav(ly, tmp, hDyu - uD2);
+	ds[7] = fmav(lz, tmp, hDzu - uD3);
 
 	aux.r = r; aux.ir = ir; aux.f = f; aux.lx = lx; aux.ly = ly; aux.lz = lz;
 	aux.flu = flu; aux.iss = iss;
+	(void)one;
 }
 
-/* Torus flow + transfer in FP32 (same model as the FP64 kernel). */
-template <int NF>
+/* Torus flow + transfer (same model as the FP64 kernel), branch-free: the
+ * emission is masked to zero outside r_isco, where the Keplerian flow is not
+ * timelike, or where the shift is not positive. */
+template <typename V, int NF>
 __device__ __forceinline__ void
-torus_rt32(const MixedRender &c, const float *s, const Aux32 &x, float *ds)
+torus_rt(const RC<V, NF> &c, const V *s, const Aux<V> &x, V *ds)
 {
-	constexpr float LOG2E = 1.4426950408889634f;
-	float n = 0.0f, shift = 1.0f;
-	if(x.r > c.risco) {
-		const float q1 = s[1], q2 = s[2], q3 = s[3];
-		float kt = x.flu - s[4];
-		float kx = fmaf(x.flu, x.lx, s[5]);
-		float ky = fmaf(x.flu, x.ly, s[6]);
-		float R2 = fmaf(q1, q1, q2 * q2);
-		float irs = rsqrt_a(x.r);           /* r^-1/2 */
-		float sr  = x.r * irs;              /* r^1/2  */
-		float Om  = rcp_a(fmaf(x.r, sr, c.a));
-		float vv  = fmaf(Om * Om, R2, -1.0f);
-		float lv  = fmaf(-(c.a * Om * R2), x.iss, 1.0f);
-		float D   = -fmaf(x.f * lv, lv, vv);
-		if(D > 0.0f) {
-			float utf = rsqrt_a(D);
-			shift = -utf * fmaf(Om, fmaf(q1, ky, -(q2 * kx)), kt);
-			if(shift > 0.0f) {
-				/* n0 (r_+/r)^1.5 exp(-z^2 / (2 (h r)^2)) */
-				float e = ex2_a(-(q3 * q3) * (x.ir * x.ir) * c.ihr2_log2e);
-				n = c.n0_rp15 * (x.ir * irs) * e;
-			}
-		}
-	}
-	if(n == 0.0f) {
-#pragma unroll
-		for(int i = 0; i < 2 * NF; ++i)
-			ds[8 + i] = 0.0f;
-		return;
-	}
-	float ish  = rcp_a(shift);
-	float jfac = n * ex2_a(-0.7f * lg2_a(shift));
-	float tfac = c.kappa * n * ish;
-	float is2  = ish * ish;
+	typedef typename MaskOf<V>::T M;
+	const V one = bc<V>(1.0f), zero = bc<V>(0.0f);
+	const V q1 = s[1], q2 = s[2], q3 = s[3];
+	V kt  = x.flu - s[4];
+	V kx  = fmav(x.flu, x.lx, s[5]);
+	V ky  = fmav(x.flu, x.ly, s[6]);
+	V R2  = fmav(q1, q1, q2 * q2);
+	V irs = rsqv(x.r);                 /* r^-1/2 */
+	V sr  = x.r * irs;                 /* r^1/2  */
+	V Om  = rcpv(fmav(x.r, sr, c.a));
+	V vv  = fmav(Om * Om, R2, -one);
+	V lv  = fmav(-((c.a * Om) * R2), x.iss, one);
+	V D   = -fmav(x.f * lv, lv, vv);
+	M ok  = andv(gtv(x.r, c.risco), gtv(D, zero));
+	V utf = rsqv(selv(ok, D, one));
+	V shift = -(utf * fmav(Om, fmav(q1, ky, -(q2 * kx)), kt));
+	ok = andv(ok, gtv(shift, zero));
+	V sh = selv(ok, shift, one);
+	/* n0 (r_+/r)^1.5 exp(-z^2 / (2 (h r)^2)) */
+	V e = ex2v(-((q3 * q3) * ((x.ir * x.ir) * c.ihr2)));
+	V n = selv(ok, (c.n0_rp15 * c.torus) * ((x.ir * irs) * e), zero);
+	V ish  = rcpv(sh);
+	V jfac = n * ex2v(bc<V>(-0.7f) * lg2v(sh));
+	V tfac = (c.kappa * n) * ish;
+	V is2  = ish * ish;
+	const V mlog2e = bc<V>(-1.4426950408889634f);
 #pragma unroll
 	for(int i = 0; i < NF; ++i) {
-		float j = jfac * c.nupow[i];
-		ds[8 + i]      = -(j * ex2_a(-s[8 + NF + i] * LOG2E)) * is2;
+		V j = jfac * c.nupow[i];
+		ds[8 + i]      = -((j * ex2v(s[8 + NF + i] * mlog2e)) * is2);
 		ds[8 + NF + i] = -(tfac * c.nuinv2[i]);
 	}
 }
 
-template <int NF>
+template <typename V, int NF>
 __device__ __forceinline__ void
-rhs32(const MixedRender &c, const float *s, float *ds)
+rhs(const RC<V, NF> &c, const V *s, V *ds)
 {
-	Aux32 aux;
-	ks_rhs32(c, s, ds, aux);
-	if(NF > 0) {
-		if(c.flow == GRAY_FLOW_TORUS) {
-			torus_rt32<NF>(c, s, aux, ds);
-		} else {
-#pragma unroll
-			for(int i = 0; i < 2 * NF; ++i)
-				ds[8 + i] = 0.0f;
-		}
-	}
+	Aux<V> aux;
+	ks_rhs<V, NF>(c, s, ds, aux);
+	if(NF > 0)
+		torus_rt<V, NF>(c, s, aux, ds);
 }
 
-/* FP64 radius root (KS.cl:48-55) for the near-horizon island */
+/* ---------------------------------------------------------- FP64 islands */
+
+/* KS.cl:48-55 radius root */
 __device__ __forceinline__ double
 getrr_d(double aa, double x, double y, double z)
 {
@@ -243,7 +336,7 @@ getrr_d(double aa, double x, double y, double z)
 	return sqrt(fma(kk, kk, aa * zz)) + kk;
 }
 
-/* FP64 null-constraint check from the final state (KS.cl:164-168) */
+/* KS.cl:164-168 null constraint from the final state */
 __device__ __forceinline__ double
 getuu_d(double a, const double *s)
 {
@@ -266,63 +359,49 @@ getuu_d(double a, const double *s)
 	return fma(k3, s[7], fma(k2, s[6], fma(k1, s[5], k0 * s[4])));
 }
 
-/* Per-lane state of the ray being integrated. */
-template <int ND>
-struct Lane {
-	float hi[ND], lo[ND]; /* compensated state: value = hi - lo          */
-	int   render;         /* index into the render table                 */
-	long long ray;        /* ray index within its render                 */
-	int   dump;           /* current dump interval                       */
-	int   h;              /* ticks done in this interval                 */
-	int   dh_cap;         /* ticks of a capped step (|dt| / n_sub)       */
-	float cdt;            /* n / |dt|: ticks per unit affine length      */
-	float dtn;            /* dt / n: affine length of one tick (signed)  */
+/* ------------------------------------------------------ slot bookkeeping */
+
+/* Scalar state of one ray slot (a thread has Lanes<V>::N slots). */
+struct Slot {
+	const MixedRender *c;
+	long long ray;
+	int dump, dump_end, h, n, dh_cap;
+	float cdt;   /* n / |dt| */
+	float dtn;   /* dt / n   */
+	float rp, eps_stop, cdt_scale;
+	double aa_d, rp_d;
+	bool active;
 };
 
 /* Per-dump constants, computed in FP64 exactly like the host loop of
  * sim-org/gray.c:251-252 and driver.cl:93. */
-template <int ND>
 __device__ __forceinline__ void
-start_dump(const MixedRender &c, Lane<ND> &L, int n)
+start_dump(Slot &S)
 {
-	double t      = c.t_init + (double)L.dump * c.dt_dump;
-	double target = c.t_init + (double)(L.dump + 1) * c.dt_dump;
+	const MixedRender &c = *S.c;
+	double t      = c.t_init + (double)S.dump * c.dt_dump;
+	double target = c.t_init + (double)(S.dump + 1) * c.dt_dump;
 	double dt     = target - t;
 	double dts    = dt / (double)c.n_sub;
-	L.dh_cap = (int)(dts / dt * (double)n);
-	L.cdt    = (float)((double)n / fabs(dt));
-	L.dtn    = (float)(dt / (double)n);
-	L.h      = 0;
+	S.dh_cap = (int)(dts / dt * (double)S.n);
+	S.cdt    = (float)((double)S.n / fabs(dt));
+	S.dtn    = (float)(dt / (double)S.n);
+	S.h      = 0;
 }
 
-template <int ND>
+template <typename V, int ND>
 __device__ __forceinline__ void
-load_ray(const MixedRender &c, Lane<ND> &L, int n)
+store_slot(const Slot &S, int k, const V *hi, const V *lo)
 {
-	const long long nr = c.n_rays;
-#pragma unroll
-	for(int k = 0; k < ND; ++k) {
-		double v = c.data[k * nr + L.ray];
-		float hi = (float)v;
-		L.hi[k] = hi;
-		L.lo[k] = (float)((double)hi - v);
-	}
-	L.dump = 0;
-	start_dump(c, L, n);
-}
-
-template <int ND>
-__device__ __forceinline__ void
-store_ray(const MixedRender &c, const Lane<ND> &L)
-{
+	const MixedRender &c = *S.c;
 	const long long nr = c.n_rays;
 	double s[ND];
 #pragma unroll
-	for(int k = 0; k < ND; ++k) {
-		s[k] = (double)L.hi[k] - (double)L.lo[k];
-		c.data[k * nr + L.ray] = s[k];
+	for(int i = 0; i < ND; ++i) {
+		s[i] = (double)getl(hi[i], k) - (double)getl(lo[i], k);
+		c.data[i * nr + S.ray] = s[i];
 	}
-	c.info[L.ray] = getuu_d(c.a_d, s);
+	c.info[S.ray] = getuu_d(c.a_d, s);
 }
 
 /* Map a global queue index to (render, ray) by binary search over the
@@ -341,123 +420,183 @@ find_render(const MixedTable &T, unsigned long long g)
 	return lo;
 }
 
-template <int NF>
-__global__ void __launch_bounds__(256)
+/* Step size of slot k in ticks (phys.cl:48-64 via driver.cl:93), with the
+ * FP64 island near r_+; 0 means the ray stops (captured or NaN). */
+template <typename V>
+__device__ __forceinline__ int
+ticks(const Slot &S, int k, const V *hi, const V *lo)
+{
+	float x = getl(hi[1], k), y = getl(hi[2], k), z = getl(hi[3], k);
+	float aa = (float)S.aa_d;
+	float zz = z * z;
+	float kk = 0.5f * (fmaf(x, x, fmaf(y, y, zz)) - aa);
+	float rr = sqrt_a(fmaf(kk, kk, aa * zz)) + kk;
+	float eps = sqrt_a(rr) - S.rp;
+	if(eps < 1.0f) {
+		double xd = (double)x - (double)getl(lo[1], k);
+		double yd = (double)y - (double)getl(lo[2], k);
+		double zd = (double)z - (double)getl(lo[3], k);
+		eps = (float)(sqrt(getrr_d(S.aa_d, xd, yd, zd)) - S.rp_d);
+	}
+	if(!(eps >= S.eps_stop))
+		return 0;
+	float want = S.cdt_scale * eps * eps * S.cdt; /* 0.01 eps^2 n / |dt| */
+	int dh = want < (float)S.dh_cap ? (int)want : S.dh_cap;
+	return dh < S.n - S.h ? dh : S.n - S.h;
+}
+
+template <int NF, typename V>
+__global__ void __launch_bounds__(Lanes<V>::N == 1 ? 256 : 128)
 mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
              unsigned long long *__restrict__ steps)
 {
 	constexpr int ND = 8 + 2 * NF;
+	constexpr int L = Lanes<V>::N;
 	const unsigned FULL = 0xffffffffu;
 	const int lane = threadIdx.x & 31;
 
-	Lane<ND> L;
-	bool active = false, exhausted = false;
+	V hi[ND], lo[ND];
+	RC<V, NF> rc;
+	Slot S[L];
+	bool exhausted = false;
 	unsigned long long cnt = 0;
-	const MixedRender *c = nullptr;
-	int n = 0;
+#pragma unroll
+	for(int k = 0; k < L; ++k)
+		S[k].active = false;
+#pragma unroll
+	for(int i = 0; i < ND; ++i) {
+		hi[i] = bc<V>(0.0f);
+		lo[i] = bc<V>(0.0f);
+	}
+	rc = RC<V, NF>();
 
 	for(;;) {
-		/* refill the lanes whose ray finished (warp-ballot compaction) */
-		bool need = !active && !exhausted;
-		unsigned mask = __ballot_sync(FULL, need);
-		if(mask) {
+		/* refill the slots whose ray finished (warp-ballot compaction) */
+#pragma unroll
+		for(int k = 0; k < L; ++k) {
+			bool need = !S[k].active && !exhausted;
+			unsigned mask = __ballot_sync(FULL, need);
+			if(!mask)
+				continue;
 			int leader = __ffs(mask) - 1;
 			unsigned base = 0;
 			if(lane == leader)
 				base = atomicAdd(queue, (unsigned)__popc(mask));
 			base = __shfl_sync(FULL, base, leader);
-			if(need) {
-				unsigned long long g = (unsigned long long)base +
-				                       __popc(mask & ((1u << lane) - 1));
-				if(g < T.total) {
-					L.render = find_render(T, g);
-					c = &T.renders[L.render];
-					L.ray = (long long)(g - T.prefix[L.render]);
-					n = (int)((INT_MAX / c->n_sub) * c->n_sub);
-					load_ray(*c, L, n);
-					active = true;
-				} else {
-					exhausted = true;
-				}
+			if(!need)
+				continue;
+			unsigned long long g = (unsigned long long)base + __popc(mask & ((1u << lane) - 1));
+			if(g >= T.total) {
+				exhausted = true;
+				continue;
+			}
+			int rdx = find_render(T, g);
+			const MixedRender &c = T.renders[rdx];
+			Slot &s = S[k];
+			s.c = &c;
+			s.ray = (long long)(g - T.prefix[rdx]);
+			s.n = (int)((INT_MAX / c.n_sub) * c.n_sub);
+			s.dump = c.dump_begin;
+			s.dump_end = c.dump_end;
+			s.rp = c.rp;
+			s.eps_stop = c.eps_stop;
+			s.cdt_scale = c.cdt_scale;
+			s.aa_d = c.aa_d;
+			s.rp_d = c.rp_d;
+			load_rc<V, NF>(rc, k, c);
+			const long long nr = c.n_rays;
+#pragma unroll
+			for(int i = 0; i < ND; ++i) {
+				double v = c.data[i * nr + s.ray];
+				float h = (float)v;
+				setl(hi[i], k, h);
+				setl(lo[i], k, (float)((double)h - v));
+			}
+			if(s.dump >= s.dump_end) { /* empty window: state unchanged */
+				store_slot<V, ND>(s, k, hi, lo);
+				continue;
+			}
+			start_dump(s);
+			s.active = true;
+		}
+		bool any = false;
+#pragma unroll
+		for(int k = 0; k < L; ++k)
+			any |= S[k].active;
+		if(!__any_sync(FULL, any))
+			break;
+
+		/* step control per slot; finished slots store and free */
+		int dh[L];
+		bool step = false;
+#pragma unroll
+		for(int k = 0; k < L; ++k) {
+			dh[k] = 0;
+			if(!S[k].active)
+				continue;
+			dh[k] = ticks<V>(S[k], k, hi, lo);
+			if(dh[k] == 0) {
+				store_slot<V, ND>(S[k], k, hi, lo);
+				S[k].active = false;
+			} else {
+				step = true;
 			}
 		}
-		if(!__any_sync(FULL, active))
-			break;
-		if(!active)
+		if(!step)
 			continue;
-
-		/* step control: phys.cl:48-64 with the FP64 island near r_+ */
-		float rr32 = 0.0f;
-		{
-			float zz = L.hi[3] * L.hi[3];
-			float kk = 0.5f * (fmaf(L.hi[1], L.hi[1], fmaf(L.hi[2], L.hi[2], zz)) - c->aa);
-			rr32 = sqrt_a(fmaf(kk, kk, c->aa * zz)) + kk;
-		}
-		float eps = sqrt_a(rr32) - c->rp;
-		if(eps < 1.0f) {
-			double x = (double)L.hi[1] - (double)L.lo[1];
-			double y = (double)L.hi[2] - (double)L.lo[2];
-			double z = (double)L.hi[3] - (double)L.lo[3];
-			eps = (float)(sqrt(getrr_d(c->aa_d, x, y, z)) - c->rp_d);
-		}
-		int dh;
-		if(!(eps >= c->eps_stop)) { /* captured (or NaN): ray done */
-			dh = 0;
-		} else {
-			float want = c->cdt_scale * eps * eps * L.cdt; /* 0.01 eps^2 n / |dt| */
-			dh = want < (float)L.dh_cap ? (int)want : L.dh_cap;
-		}
-		if(dh == 0) {
-			store_ray(*c, L);
-			active = false;
-			continue;
-		}
-		if(dh > n - L.h)
-			dh = n - L.h;
 
 		/* RK4.cl:37-47 with the compensated update */
+		V hs;
+#pragma unroll
+		for(int k = 0; k < L; ++k)
+			setl(hs, k, (float)dh[k] * S[k].dtn);
+		const V hh = bc<V>(0.5f) * hs;
 		{
-			const float hs  = (float)dh * L.dtn;
-			const float hh  = 0.5f * hs;
-			float k[ND], t[ND], sum[ND];
-			rhs32<NF>(*c, L.hi, k);
+			V kk[ND], t[ND], sum[ND];
+			rhs<V, NF>(rc, hi, kk);
 #pragma unroll
 			for(int i = 0; i < ND; ++i) {
-				sum[i] = k[i];
-				t[i] = fmaf(hh, k[i], L.hi[i]);
+				sum[i] = kk[i];
+				t[i] = fmav(hh, kk[i], hi[i]);
 			}
-			rhs32<NF>(*c, t, k);
+			rhs<V, NF>(rc, t, kk);
 #pragma unroll
 			for(int i = 0; i < ND; ++i) {
-				sum[i] = fmaf(2.0f, k[i], sum[i]);
-				t[i] = fmaf(hh, k[i], L.hi[i]);
+				sum[i] = fmav(bc<V>(2.0f), kk[i], sum[i]);
+				t[i] = fmav(hh, kk[i], hi[i]);
 			}
-			rhs32<NF>(*c, t, k);
+			rhs<V, NF>(rc, t, kk);
 #pragma unroll
 			for(int i = 0; i < ND; ++i) {
-				sum[i] = fmaf(2.0f, k[i], sum[i]);
-				t[i] = fmaf(hs, k[i], L.hi[i]);
+				sum[i] = fmav(bc<V>(2.0f), kk[i], sum[i]);
+				t[i] = fmav(hs, kk[i], hi[i]);
 			}
-			rhs32<NF>(*c, t, k);
-			const float h6 = hs * (1.0f / 6.0f);
+			rhs<V, NF>(rc, t, kk);
+			const V h6 = hs * bc<V>(1.0f / 6.0f);
 #pragma unroll
 			for(int i = 0; i < ND; ++i) {
-				float inc = h6 * (sum[i] + k[i]);
+				V inc = h6 * (sum[i] + kk[i]);
 				/* Kahan: value = hi - lo */
-				float yv = inc - L.lo[i];
-				float tv = L.hi[i] + yv;
-				L.lo[i] = (tv - L.hi[i]) - yv;
-				L.hi[i] = tv;
+				V yv = inc - lo[i];
+				V tv = hi[i] + yv;
+				lo[i] = (tv - hi[i]) - yv;
+				hi[i] = tv;
 			}
 		}
-		++cnt;
-		L.h += dh;
-		if(L.h >= n) {
-			if(++L.dump >= c->n_dump) {
-				store_ray(*c, L);
-				active = false;
-			} else {
-				start_dump(*c, L, n);
+#pragma unroll
+		for(int k = 0; k < L; ++k) {
+			if(dh[k] == 0)
+				continue;
+			++cnt;
+			Slot &s = S[k];
+			s.h += dh[k];
+			if(s.h >= s.n) {
+				if(++s.dump >= s.dump_end) {
+					store_slot<V, ND>(s, k, hi, lo);
+					s.active = false;
+				} else {
+					start_dump(s);
+				}
 			}
 		}
 	}
@@ -469,28 +608,57 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 		atomicAdd(steps, cnt);
 }
 
-template <int NF>
+template <int NF, typename V>
 cudaError_t
 launch_nf(const MixedTable &T, unsigned int *queue, unsigned long long *steps,
           cudaStream_t st, const MixedLaunch &cfg)
 {
-	int block = cfg.block > 0 ? cfg.block : 256;
+	const int maxb = Lanes<V>::N == 1 ? 256 : 128;
+	int block = cfg.block > 0 ? cfg.block : maxb;
+	if(block > maxb || block % 32)
+		return cudaErrorInvalidValue;
 	int per_sm = cfg.blocks_per_sm;
-	if(per_sm <= 0) {
-		cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-			&per_sm, mixed_kernel<NF>, block, 0);
-		if(e != cudaSuccess)
-			return e;
-		if(per_sm <= 0)
-			per_sm = 1;
-	}
+	int occ = 0;
+	cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mixed_kernel<NF, V>,
+	                                                              block, 0);
+	if(e != cudaSuccess)
+		return e;
+	if(per_sm <= 0 || per_sm > occ)
+		per_sm = occ > 0 ? occ : 1;
+	const unsigned long long rays_per_block = (unsigned long long)block * Lanes<V>::N;
 	long long want = (long long)per_sm * (cfg.sms > 0 ? cfg.sms : 148);
-	long long need = (long long)((T.total + block - 1) / block);
+	long long need = (long long)((T.total + rays_per_block - 1) / rays_per_block);
 	unsigned grid = (unsigned)(want < need ? want : need);
 	if(grid == 0)
 		grid = 1;
-	mixed_kernel<NF><<<grid, block, 0, st>>>(T, queue, steps);
+	mixed_kernel<NF, V><<<grid, block, 0, st>>>(T, queue, steps);
 	return cudaGetLastError();
+}
+
+template <typename V>
+cudaError_t
+launch_v(const MixedTable &T, int n_freq, unsigned int *queue, unsigned long long *steps,
+         cudaStream_t st, const MixedLaunch &cfg)
+{
+	switch(n_freq) {
+	case 0: return launch_nf<0, V>(T, queue, steps, st, cfg);
+	case 1: return launch_nf<1, V>(T, queue, steps, st, cfg);
+	case 2: return launch_nf<2, V>(T, queue, steps, st, cfg);
+	case 3: return launch_nf<3, V>(T, queue, steps, st, cfg);
+	case 4: return launch_nf<4, V>(T, queue, steps, st, cfg);
+	case 5: return launch_nf<5, V>(T, queue, steps, st, cfg);
+	case 6: return launch_nf<6, V>(T, queue, steps, st, cfg);
+	case 7: return launch_nf<7, V>(T, queue, steps, st, cfg);
+	case 8: return launch_nf<8, V>(T, queue, steps, st, cfg);
+	default: return cudaErrorInvalidValue;
+	}
+}
+
+template <int NF, typename V>
+cudaError_t
+occ_nf(int block, int *out)
+{
+	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, mixed_kernel<NF, V>, block, 0);
 }
 
 } /* namespace */
@@ -502,18 +670,30 @@ launch_mixed_table(const MixedTable &T, int n_freq, unsigned int *queue,
 	cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned int), st);
 	if(e != cudaSuccess)
 		return e;
+	if(cfg.rays_per_thread == 2)
+		return launch_v<F2>(T, n_freq, queue, steps, st, cfg);
+	return launch_v<float>(T, n_freq, queue, steps, st, cfg);
+}
+
+cudaError_t
+mixed_occupancy(int n_freq, const MixedLaunch &cfg, int *blocks_per_sm)
+{
+	const bool two = cfg.rays_per_thread == 2;
+	const int block = cfg.block > 0 ? cfg.block : (two ? 128 : 256);
+#define OCC(NF) (two ? occ_nf<NF, F2>(block, blocks_per_sm) : occ_nf<NF, float>(block, blocks_per_sm))
 	switch(n_freq) {
-	case 0: return launch_nf<0>(T, queue, steps, st, cfg);
-	case 1: return launch_nf<1>(T, queue, steps, st, cfg);
-	case 2: return launch_nf<2>(T, queue, steps, st, cfg);
-	case 3: return launch_nf<3>(T, queue, steps, st, cfg);
-	case 4: return launch_nf<4>(T, queue, steps, st, cfg);
-	case 5: return launch_nf<5>(T, queue, steps, st, cfg);
-	case 6: return launch_nf<6>(T, queue, steps, st, cfg);
-	case 7: return launch_nf<7>(T, queue, steps, st, cfg);
-	case 8: return launch_nf<8>(T, queue, steps, st, cfg);
+	case 0: return OCC(0);
+	case 1: return OCC(1);
+	case 2: return OCC(2);
+	case 3: return OCC(3);
+	case 4: return OCC(4);
+	case 5: return OCC(5);
+	case 6: return OCC(6);
+	case 7: return OCC(7);
+	case 8: return OCC(8);
 	default: return cudaErrorInvalidValue;
 	}
+#undef OCC
 }
 
 void
@@ -535,6 +715,8 @@ fill_mixed_render(const RenderParams &p, double *data, double *info, double t_in
 		m->nuinv2[i] = p.nuinv2_f[i];
 	}
 	m->flow = p.flow;
+	m->dump_begin = 0;
+	m->dump_end = (int)n_dump;
 	m->a_d = p.a;
 	m->aa_d = p.aa;
 	m->rp_d = p.rp;
@@ -543,6 +725,5 @@ fill_mixed_render(const RenderParams &p, double *data, double *info, double t_in
 	m->n_rays = p.n_rays;
 	m->t_init = t_init;
 	m->dt_dump = dt_dump;
-	m->n_dump = (int)n_dump;
 	m->n_sub = n_sub;
 }

@@ -16,11 +16,12 @@ struct MixedRender {
 	float  nupow[GRAY_MAX_FREQ];
 	float  nuinv2[GRAY_MAX_FREQ];
 	int    flow;
-	int    n_dump;
+	int    dump_begin;         /* integrate dump intervals [dump_begin,        */
+	int    dump_end;           /*   dump_end) of the render's schedule          */
 	double a_d, aa_d, rp_d;    /* FP64 islands                                */
 	double *data, *info;       /* SoA FP64 state and getuu diagnostic         */
 	long long n_rays;
-	double t_init, dt_dump;
+	double t_init, dt_dump;    /* dump i covers [t_init + i dt, t_init + (i+1) dt] */
 	long long n_sub;
 };
 
@@ -35,6 +36,7 @@ void fill_mixed_render(const RenderParams &p, double *data, double *info,
                        double t_init, double dt_dump, long long n_dump,
                        long long n_sub, MixedRender *m);
 
+/* rays_per_thread: 1 (scalar FP32) or 2 (two rays per thread in f32x2) */
 cudaError_t launch_mixed_table(const MixedTable &T, int n_freq, unsigned int *queue,
                                unsigned long long *steps, cudaStream_t st,
                                const MixedLaunch &cfg);
@@ -43,5 +45,8 @@ cudaError_t launch_mixed_table(const MixedTable &T, int n_freq, unsigned int *qu
 cudaError_t launch_dyst_mixed_table(const MixedTable &T, const GridParams &g,
                                     unsigned int *queue, unsigned long long *steps,
                                     cudaStream_t st, const MixedLaunch &cfg);
+
+/* resident blocks per SM of the mixed kernel for a launch shape */
+cudaError_t mixed_occupancy(int n_freq, const MixedLaunch &cfg, int *blocks_per_sm);
 
 #endif /* GRAY_MIXED_TABLE_H */

@@ -131,7 +131,8 @@ gray_run_mixed_noalloc(int device, const gray_render_desc *descs, int n_renders,
 		T.prefix = S->prefix;
 		T.n_renders = n_renders;
 		T.total = total;
-		MixedLaunch cfg = {256, 0, sms};
+		/* the context's default plan: one ray per thread, 256 threads */
+		MixedLaunch cfg = {256, 0, sms, 1};
 		e = launch_mixed_table(T, n_freq, &S->queue, &S->steps, st, cfg);
 	}
 	if(e == cudaSuccess && steps_host) {

@@ -163,6 +163,43 @@ int gray_read_kdown(gray_ctx *ctx, int render_id, double *k, size_t bytes);
 /* Accepted RK4 steps summed over the render's rays since the last icond. */
 int gray_ray_steps(gray_ctx *ctx, int render_id, uint64_t *steps);
 
+/* ---- batches, launch plans, graphs ---------------------------------- */
+
+/* A batch is many mixed-precision renders integrated by ONE persistent
+ * launch (a render table; rays of every render share the warp-refilled ray
+ * queue).  The first gray_batch_run captures the sequence -- per-render
+ * initial conditions, queue reset, persistent kernel -- into a CUDA graph;
+ * later runs replay it.  All renders of a batch use the same spacetime;
+ * analytic ones also the same n_freq.  Renders stay owned by the context
+ * and must outlive the batch. */
+int gray_batch_create(gray_ctx *ctx, const int *render_ids, int n, int *batch_id);
+int gray_batch_destroy(gray_ctx *ctx, int batch_id);
+int gray_batch_run(gray_ctx *ctx, int batch_id, double *ns);
+int gray_batch_steps(gray_ctx *ctx, int batch_id, uint64_t *steps);
+
+/* Launch shape of the persistent kernels. */
+typedef struct gray_launch_plan {
+	int32_t block;            /* threads per block                          */
+	int32_t blocks_per_sm;    /* 0 = as many as fit                         */
+	int32_t rays_per_thread;  /* 1 (scalar FP32) or 2 (packed f32x2)         */
+	double  ns;               /* measured trial time (gray_plan output)      */
+} gray_launch_plan;
+
+enum gray_plan_flags {
+	GRAY_PLAN_ESTIMATE = 0,   /* choose by rule, no trial launches          */
+	GRAY_PLAN_MEASURE  = 1    /* time every candidate on the batch           */
+};
+
+/* Autotuner replacing the lux planner of sim/gray/Kerr/ocl.c:41-75 and
+ * tests/ck_sample.c:84-104 (7 work-group sizes, estimate or measure): picks
+ * block size, blocks per SM and rays per thread for the batch's kernel,
+ * installs it in the context and returns it.  MEASURE runs trial launches
+ * over the first dump intervals of the batch, leaving the renders' state
+ * undefined (gray_batch_run / gray_run start from icond again). */
+int gray_plan(gray_ctx *ctx, int batch_id, int flags, gray_launch_plan *best);
+int gray_set_plan(gray_ctx *ctx, const gray_launch_plan *plan);
+int gray_get_plan(const gray_ctx *ctx, gray_launch_plan *plan);
+
 /* ---- numerical spacetime (sim-org/io.c:302-533, interp.cl, dyst.cl) - */
 
 typedef struct gray_grid_desc {
