@@ -34,7 +34,10 @@ EXPORTS = [
     "gray_run_mixed_noalloc", "gray_read_spacetime",
     "gray_batch_create", "gray_batch_destroy", "gray_batch_run", "gray_batch_steps",
     "gray_plan", "gray_set_plan", "gray_get_plan",
+    "gray_serve_clock", "gray_serve_start", "gray_serve_submit", "gray_serve_poll",
+    "gray_serve_result", "gray_serve_cancel", "gray_serve_get_stats", "gray_serve_stop",
 ]
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED, REQ_CANCELLED = 0, 1, 2, 3, 4
 PLAN_ESTIMATE, PLAN_MEASURE = 0, 1
 NOALLOC_MAX_RENDERS = 32
 
@@ -70,6 +73,23 @@ class LaunchPlan(ctypes.Structure):
     def as_dict(self):
         return {"block": self.block, "blocks_per_sm": self.blocks_per_sm,
                 "rays_per_thread": self.rays_per_thread, "trial_ns": self.ns}
+
+
+class ServeConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_size_t), ("max_inflight", ctypes.c_int32),
+                ("dumps_per_iter", ctypes.c_int32)]
+
+
+class RequestStatus(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int32), ("status", ctypes.c_int32),
+                ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double),
+                ("t_done", ctypes.c_double), ("n_rays", ctypes.c_uint64)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_uint64), ("ray_steps", ctypes.c_uint64 * 2),
+                ("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+                ("cancelled", ctypes.c_uint64), ("busy_s", ctypes.c_double)]
 
 
 class GridDesc(ctypes.Structure):
@@ -157,6 +177,15 @@ def lib():
         L.gray_plan.argtypes = [vp, i, i, P(LaunchPlan)]
         L.gray_set_plan.argtypes = [vp, P(LaunchPlan)]
         L.gray_get_plan.argtypes = [vp, P(LaunchPlan)]
+        L.gray_serve_clock.restype = d
+        L.gray_serve_clock.argtypes = []
+        L.gray_serve_start.argtypes = [vp, P(ServeConfig)]
+        L.gray_serve_submit.argtypes = [vp, P(RenderDesc), P(u64)]
+        L.gray_serve_poll.argtypes = [vp, u64, P(RequestStatus)]
+        L.gray_serve_result.argtypes = [vp, u64, vp, sz, vp, sz]
+        L.gray_serve_cancel.argtypes = [vp, u64]
+        L.gray_serve_get_stats.argtypes = [vp, P(ServeStats)]
+        L.gray_serve_stop.argtypes = [vp, i]
         _lib = L
     return _lib
 
@@ -338,6 +367,48 @@ class Context:
         p = LaunchPlan()
         _ck(lib().gray_get_plan(self.h, ctypes.byref(p)), "gray_get_plan")
         return p
+
+    # ---- serving (continuous batching)
+    def serve_start(self, hbm_budget=0, max_inflight=0, dumps_per_iter=0):
+        cfg = ServeConfig(hbm_budget, max_inflight, dumps_per_iter)
+        _ck(lib().gray_serve_start(self.h, ctypes.byref(cfg)), "gray_serve_start")
+
+    def submit(self, cfg):
+        d = make_desc(dict(cfg, precision=cfg.get("precision", PREC_MIXED)))
+        rid = ctypes.c_uint64(0)
+        _ck(lib().gray_serve_submit(self.h, ctypes.byref(d), ctypes.byref(rid)), "gray_serve_submit")
+        return rid.value
+
+    def poll(self, rid):
+        s = RequestStatus()
+        _ck(lib().gray_serve_poll(self.h, rid, ctypes.byref(s)), "gray_serve_poll")
+        return s
+
+    def result(self, rid, n_data, n_rays):
+        data = np.empty((n_data, n_rays), dtype=np.float64)
+        info = np.empty(n_rays, dtype=np.float64)
+        _ck(lib().gray_serve_result(self.h, rid, data.ctypes.data, data.nbytes,
+                                    info.ctypes.data, info.nbytes), "gray_serve_result")
+        return data, info
+
+    def release(self, rid):
+        """Drop a finished / failed / cancelled request; returns its status."""
+        return lib().gray_serve_result(self.h, rid, None, 0, None, 0)
+
+    def cancel(self, rid):
+        _ck(lib().gray_serve_cancel(self.h, rid), "gray_serve_cancel")
+
+    def serve_stats(self):
+        s = ServeStats()
+        st = lib().gray_serve_get_stats(self.h, ctypes.byref(s))
+        return s, st
+
+    def serve_stop(self, drain=False):
+        return lib().gray_serve_stop(self.h, 1 if drain else 0)
+
+    @staticmethod
+    def clock():
+        return lib().gray_serve_clock()
 
     def read_spacetime(self, grid, level):
         out = np.empty((grid.nz, grid.ny, grid.nx, 51), dtype=np.float32)

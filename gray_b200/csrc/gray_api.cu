@@ -12,68 +12,7 @@
 #include <new>
 #include <vector>
 
-#include "gray_internal.h"
-#include "mixed_table.h"
-
-struct Render {
-	gray_render_desc desc;
-	RenderParams p;
-	double *d_data = nullptr;
-	double *d_info = nullptr;
-	unsigned long long *d_steps = nullptr;
-	unsigned int *d_queue = nullptr;
-	MixedRender *d_table = nullptr;       /* one-entry table for gray_run */
-	unsigned long long *d_prefix = nullptr;
-	size_t bytes = 0;
-	bool has_state = false;
-};
-
-struct Grid {
-	gray_grid_desc desc;
-	bool loaded[2] = {false, false};
-	float *lvl[2] = {nullptr, nullptr};
-	double *nodes[3] = {nullptr, nullptr, nullptr};
-	float *nodes_f[3] = {nullptr, nullptr, nullptr};
-	size_t bytes = 0;
-	GridParams gp;
-};
-
-struct Batch {
-	std::vector<int> ids;
-	int spacetime = GRAY_ST_KERR;
-	int n_freq = 0;
-	unsigned long long total = 0;
-	void *block = nullptr;          /* table | prefix | queue | steps      */
-	size_t bytes = 0;
-	MixedRender *d_table = nullptr;
-	unsigned long long *d_prefix = nullptr;
-	unsigned int *d_queue = nullptr;
-	unsigned long long *d_steps = nullptr;
-	std::vector<MixedRender> host_table;
-	cudaGraphExec_t exec = nullptr;
-	MixedLaunch graph_cfg = {0, 0, 0, 0};
-	cudaStream_t graph_stream = nullptr;
-};
-
-struct gray_ctx {
-	int device = 0;
-	size_t budget = 0;
-	size_t used = 0;
-	int sms = 0;
-	cudaStream_t own = nullptr;
-	cudaStream_t stream = nullptr;
-	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-	std::map<int, Render *> renders;
-	int next_id = 1;
-	Grid *grid = nullptr;
-	int evolve64_block = 128;
-	/* default plan (GRAY_PLAN_ESTIMATE): one ray per thread, 256-thread
-	 * blocks -- the shape the measuring planner picks on B200 for the
-	 * analytic torus renders */
-	MixedLaunch mixed = {256, 0, 0, 1};
-	std::map<int, Batch *> batches;
-	int next_batch = 1;
-};
+#include "ctx_internal.h"
 
 namespace {
 
@@ -97,6 +36,7 @@ from_cuda(cudaError_t e)
 int
 dalloc(gray_ctx *c, void **p, size_t bytes)
 {
+	std::lock_guard<std::mutex> lk(c->mem_mu);
 	if(c->used + bytes > c->budget)
 		return GRAY_EBUDGET;
 	cudaError_t e = cudaMalloc(p, bytes);
@@ -113,6 +53,7 @@ void
 dfree(gray_ctx *c, void *p, size_t bytes)
 {
 	if(p) {
+		std::lock_guard<std::mutex> lk(c->mem_mu);
 		cudaFree(p);
 		c->used -= bytes;
 	}
@@ -238,7 +179,31 @@ grid_ready(gray_ctx *c)
 
 } /* namespace */
 
-/* Shared with other translation units through gray_internal.h. */
+/* Shared with other translation units (ctx_internal.h, gray_internal.h). */
+int
+gi_from_cuda(cudaError_t e)
+{
+	return from_cuda(e);
+}
+
+int
+gi_dalloc(gray_ctx *c, void **p, size_t bytes)
+{
+	return dalloc(c, p, bytes);
+}
+
+void
+gi_dfree(gray_ctx *c, void *p, size_t bytes)
+{
+	dfree(c, p, bytes);
+}
+
+int
+gi_grid_ready(gray_ctx *c)
+{
+	return grid_ready(c);
+}
+
 int
 gray_internal_check_desc(const gray_render_desc *d)
 {
@@ -352,6 +317,7 @@ gray_destroy(gray_ctx *c)
 {
 	if(!c)
 		return;
+	gi_serve_shutdown(c);
 	cudaSetDevice(c->device);
 	if(c->stream)
 		cudaStreamSynchronize(c->stream);

@@ -1,0 +1,568 @@
+/*
+ * Continuous-batching render server.
+ *
+ * A scheduler thread owns two streams.  Each iteration it
+ *   1. admits queued requests (FIFO) while the admitted state fits the HBM
+ *      budget and the table has room: allocates their state and launches
+ *      their camera initial conditions;
+ *   2. builds one render table per kind -- analytic renders grouped by
+ *      n_freq, numerical renders on the context's grid -- each entry with
+ *      the next window of dump intervals, and runs one persistent launch
+ *      per group (analytic on one stream, numerical on the other);
+ *   3. advances the windows; renders whose last interval is done are copied
+ *      to host memory and their device state freed, which lets queued
+ *      requests in on the next iteration.
+ * Requests therefore join while others are mid-render and their rays share
+ * the persistent launches.  Every entry point but the scheduler's own work
+ * takes the server mutex only briefly.
+ */
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include "ctx_internal.h"
+
+namespace {
+
+constexpr int GROUPS = GRAY_MAX_FREQ + 2; /* analytic n_freq 0..8, numerical */
+constexpr int NUM_GROUP = GRAY_MAX_FREQ + 1;
+
+double
+now_s()
+{
+	using namespace std::chrono;
+	static const steady_clock::time_point t0 = steady_clock::now();
+	return duration<double>(steady_clock::now() - t0).count();
+}
+
+struct Request {
+	uint64_t id = 0;
+	gray_render_desc desc;
+	RenderParams p;
+	int state = GRAY_REQ_QUEUED;
+	int status = GRAY_OK;
+	double t_submit = 0, t_admit = 0, t_done = 0;
+	double *d_data = nullptr, *d_info = nullptr;
+	size_t bytes = 0;
+	int next_dump = 0;
+	std::atomic<bool> cancel{false}; /* set by gray_serve_cancel, read by the scheduler */
+	std::vector<double> h_data, h_info;
+
+	int group() const { return p.spacetime == GRAY_ST_NUMERICAL ? NUM_GROUP : p.n_freq; }
+};
+
+} /* namespace */
+
+struct Server {
+	gray_ctx *c = nullptr;
+	gray_serve_config cfg;
+	size_t budget = 0;
+	std::thread th;
+	std::mutex mu;
+	std::condition_variable cv;
+	bool stop = false, drain = false;
+	std::deque<Request *> pending;
+	std::map<uint64_t, Request *> reqs;
+	std::vector<Request *> inflight;
+	size_t inflight_bytes = 0;
+	uint64_t next_id = 1;
+	gray_serve_stats stats;
+	/* device: table | prefix | 2 counters per group */
+	void *dblock = nullptr;
+	size_t dbytes = 0;
+	MixedRender *d_tab = nullptr;
+	unsigned long long *d_pre = nullptr;
+	unsigned int *d_queue = nullptr;          /* [GROUPS] (64-byte spaced) */
+	unsigned long long *d_steps = nullptr;    /* [GROUPS] */
+	MixedRender *h_tab = nullptr;             /* pinned staging */
+	unsigned long long *h_pre = nullptr;
+	unsigned long long *h_steps = nullptr;
+	cudaStream_t s[2] = {nullptr, nullptr};
+	cudaEvent_t copied = nullptr, e0 = nullptr, e1 = nullptr, e2 = nullptr;
+	int thread_status = GRAY_OK;
+};
+
+namespace {
+
+void
+release(Server *S, Request *r)
+{
+	if(r->d_data) {
+		gi_dfree(S->c, r->d_data, r->bytes);
+		r->d_data = r->d_info = nullptr;
+		S->inflight_bytes -= r->bytes;
+	}
+}
+
+/* Device-side work of one iteration.  Returns a GRAY_* status. */
+int
+iterate(Server *S, std::vector<Request *> &fresh)
+{
+	gray_ctx *c = S->c;
+	cudaError_t e = cudaSuccess;
+	/* 1. admission: state + initial conditions of the fresh requests */
+	for(Request *r : fresh) {
+		int st = gi_dalloc(c, (void **)&r->d_data, r->bytes);
+		if(st) {
+			std::lock_guard<std::mutex> lk(S->mu);
+			r->state = GRAY_REQ_FAILED;
+			r->status = st;
+			r->t_done = now_s();
+			S->inflight_bytes -= r->bytes;
+			r->d_data = nullptr;
+			S->stats.failed++;
+			continue;
+		}
+		r->d_info = r->d_data + (size_t)r->p.n_rays * r->p.n_data;
+		cudaStream_t st_ = S->s[r->group() == NUM_GROUP ? 1 : 0];
+		e = r->group() == NUM_GROUP
+		        ? launch_dyst_icond(r->p, c->grid->gp, r->d_data, r->d_info, st_)
+		        : launch_icond64(r->p, r->d_data, r->d_info, st_);
+		if(e != cudaSuccess)
+			return gi_from_cuda(e);
+		r->next_dump = 0;
+		S->inflight.push_back(r);
+	}
+	if(S->inflight.empty())
+		return GRAY_OK;
+
+	/* 2. one table per group, entries with the next window of dumps */
+	const int dpi = S->cfg.dumps_per_iter;
+	int count[GROUPS] = {0}, start[GROUPS];
+	for(Request *r : S->inflight)
+		count[r->group()]++;
+	for(int g = 0, acc = 0; g < GROUPS; ++g) {
+		start[g] = acc;
+		acc += count[g];
+	}
+	int fill[GROUPS];
+	unsigned long long total[GROUPS] = {0};
+	memcpy(fill, start, sizeof(fill));
+	for(Request *r : S->inflight) {
+		int g = r->group(), k = fill[g]++;
+		MixedRender &m = S->h_tab[k];
+		memset(&m, 0, sizeof(m));
+		fill_mixed_render(r->p, r->d_data, r->d_info, r->desc.t_init, r->desc.dt_dump,
+		                  (long long)r->desc.n_dump, (long long)r->desc.n_sub, &m);
+		m.dump_begin = r->next_dump;
+		m.dump_end = std::min(r->next_dump + dpi, (int)r->desc.n_dump);
+		S->h_pre[k] = total[g];
+		total[g] += (unsigned long long)r->p.n_rays;
+	}
+	const size_t n = S->inflight.size();
+	if((e = cudaMemcpyAsync(S->d_tab, S->h_tab, n * sizeof(MixedRender), cudaMemcpyHostToDevice,
+	                        S->s[0])) != cudaSuccess ||
+	   (e = cudaMemcpyAsync(S->d_pre, S->h_pre, n * sizeof(unsigned long long),
+	                        cudaMemcpyHostToDevice, S->s[0])) != cudaSuccess ||
+	   (e = cudaMemsetAsync(S->d_steps, 0, GROUPS * sizeof(unsigned long long), S->s[0])) !=
+	       cudaSuccess ||
+	   (e = cudaEventRecord(S->copied, S->s[0])) != cudaSuccess ||
+	   (e = cudaStreamWaitEvent(S->s[1], S->copied, 0)) != cudaSuccess ||
+	   (e = cudaEventRecord(S->e0, S->s[0])) != cudaSuccess)
+		return gi_from_cuda(e);
+	MixedLaunch cfg = c->mixed;
+	cfg.sms = c->sms;
+	for(int g = 0; g < GROUPS; ++g) {
+		if(!count[g])
+			continue;
+		MixedTable T;
+		T.renders = S->d_tab + start[g];
+		T.prefix = S->d_pre + start[g];
+		T.n_renders = count[g];
+		T.total = total[g];
+		unsigned int *q = (unsigned int *)((char *)S->d_queue + 64 * g);
+		if(g == NUM_GROUP) {
+			MixedLaunch dc = cfg;
+			dc.block = 256;
+			e = launch_dyst_mixed_table(T, c->grid->gp, q, S->d_steps + g, S->s[1], dc);
+		} else {
+			e = launch_mixed_table(T, g, q, S->d_steps + g, S->s[0], cfg);
+		}
+		if(e != cudaSuccess)
+			return gi_from_cuda(e);
+	}
+	if((e = cudaEventRecord(S->e2, S->s[1])) != cudaSuccess ||
+	   (e = cudaStreamWaitEvent(S->s[0], S->e2, 0)) != cudaSuccess ||
+	   (e = cudaEventRecord(S->e1, S->s[0])) != cudaSuccess ||
+	   (e = cudaMemcpyAsync(S->h_steps, S->d_steps, GROUPS * sizeof(unsigned long long),
+	                        cudaMemcpyDeviceToHost, S->s[0])) != cudaSuccess ||
+	   (e = cudaStreamSynchronize(S->s[0])) != cudaSuccess)
+		return gi_from_cuda(e);
+	float ms = 0.0f;
+	cudaEventElapsedTime(&ms, S->e0, S->e1);
+
+	/* 3. advance windows, retire finished renders */
+	std::vector<Request *> keep, done;
+	for(Request *r : S->inflight) {
+		r->next_dump = std::min(r->next_dump + dpi, (int)r->desc.n_dump);
+		if(r->next_dump >= (int)r->desc.n_dump || r->cancel)
+			done.push_back(r);
+		else
+			keep.push_back(r);
+	}
+	for(Request *r : done) {
+		if(!r->cancel) {
+			const size_t nr = (size_t)r->p.n_rays;
+			r->h_data.resize(nr * r->p.n_data);
+			r->h_info.resize(nr);
+			if((e = cudaMemcpyAsync(r->h_data.data(), r->d_data, r->h_data.size() * sizeof(double),
+			                        cudaMemcpyDeviceToHost, S->s[0])) != cudaSuccess ||
+			   (e = cudaMemcpyAsync(r->h_info.data(), r->d_info, nr * sizeof(double),
+			                        cudaMemcpyDeviceToHost, S->s[0])) != cudaSuccess ||
+			   (e = cudaStreamSynchronize(S->s[0])) != cudaSuccess)
+				return gi_from_cuda(e);
+		}
+		std::lock_guard<std::mutex> lk(S->mu);
+		release(S, r);
+		r->t_done = now_s();
+		if(r->cancel) {
+			r->state = GRAY_REQ_CANCELLED;
+			S->stats.cancelled++;
+		} else {
+			r->state = GRAY_REQ_DONE;
+			S->stats.completed++;
+		}
+	}
+	{
+		std::lock_guard<std::mutex> lk(S->mu);
+		S->inflight.swap(keep);
+		S->stats.iterations++;
+		S->stats.busy_s += ms * 1e-3;
+		for(int g = 0; g < GROUPS; ++g)
+			S->stats.ray_steps[g == NUM_GROUP ? 1 : 0] += S->h_steps[g];
+	}
+	S->cv.notify_all();
+	return GRAY_OK;
+}
+
+void
+loop(Server *S)
+{
+	cudaSetDevice(S->c->device);
+	for(;;) {
+		std::vector<Request *> fresh;
+		{
+			std::unique_lock<std::mutex> lk(S->mu);
+			if(S->inflight.empty())
+				S->cv.wait_for(lk, std::chrono::milliseconds(20), [&] {
+					return S->stop || !S->pending.empty();
+				});
+			if(S->stop && (!S->drain || (S->pending.empty() && S->inflight.empty())))
+				break;
+			/* FIFO admission under the budget and the table size */
+			size_t slots = S->inflight.size();
+			while(!S->pending.empty() && slots < (size_t)S->cfg.max_inflight) {
+				Request *r = S->pending.front();
+				if(r->cancel) {
+					S->pending.pop_front();
+					r->state = GRAY_REQ_CANCELLED;
+					r->t_done = now_s();
+					S->stats.cancelled++;
+					continue;
+				}
+				if(S->inflight_bytes + r->bytes > S->budget)
+					break; /* wait until running renders free memory */
+				S->pending.pop_front();
+				S->inflight_bytes += r->bytes;
+				r->state = GRAY_REQ_RUNNING;
+				r->t_admit = now_s();
+				fresh.push_back(r);
+				++slots;
+			}
+		}
+		int st = iterate(S, fresh);
+		if(st) {
+			/* device failure: fail everything in flight and stop serving */
+			std::lock_guard<std::mutex> lk(S->mu);
+			S->thread_status = st;
+			for(Request *r : S->inflight) {
+				release(S, r);
+				r->state = GRAY_REQ_FAILED;
+				r->status = st;
+				S->stats.failed++;
+			}
+			S->inflight.clear();
+			for(Request *r : S->pending) {
+				r->state = GRAY_REQ_FAILED;
+				r->status = st;
+				S->stats.failed++;
+			}
+			S->pending.clear();
+			S->stop = true;
+			break;
+		}
+	}
+	S->cv.notify_all();
+}
+
+void
+free_server(Server *S)
+{
+	gray_ctx *c = S->c;
+	for(Request *r : S->inflight)
+		release(S, r);
+	for(auto &kv : S->reqs)
+		delete kv.second;
+	if(S->dblock)
+		gi_dfree(c, S->dblock, S->dbytes);
+	if(S->h_tab)
+		cudaFreeHost(S->h_tab);
+	for(int i = 0; i < 2; ++i)
+		if(S->s[i])
+			cudaStreamDestroy(S->s[i]);
+	if(S->copied) cudaEventDestroy(S->copied);
+	if(S->e0) cudaEventDestroy(S->e0);
+	if(S->e1) cudaEventDestroy(S->e1);
+	if(S->e2) cudaEventDestroy(S->e2);
+	delete S;
+}
+
+} /* namespace */
+
+void
+gi_serve_shutdown(gray_ctx *c)
+{
+	if(!c || !c->server)
+		return;
+	Server *S = c->server;
+	{
+		std::lock_guard<std::mutex> lk(S->mu);
+		S->stop = true;
+		S->drain = false;
+	}
+	S->cv.notify_all();
+	if(S->th.joinable())
+		S->th.join();
+	free_server(S);
+	c->server = nullptr;
+}
+
+extern "C" double
+gray_serve_clock(void)
+{
+	return now_s();
+}
+
+extern "C" int
+gray_serve_start(gray_ctx *c, const gray_serve_config *cfg)
+{
+	if(!c || !cfg)
+		return GRAY_EINVAL;
+	if(c->server)
+		return GRAY_ESTATE;
+	if(cfg->max_inflight < 0 || cfg->dumps_per_iter < 0 || cfg->max_inflight > (1 << 16))
+		return GRAY_EINVAL;
+	if(cudaSetDevice(c->device) != cudaSuccess)
+		return GRAY_ECUDA;
+	Server *S = new(std::nothrow) Server;
+	if(!S)
+		return GRAY_ENOMEM;
+	S->c = c;
+	S->cfg = *cfg;
+	if(!S->cfg.max_inflight)
+		S->cfg.max_inflight = 1024;
+	if(!S->cfg.dumps_per_iter)
+		S->cfg.dumps_per_iter = 1;
+	S->budget = cfg->hbm_budget ? cfg->hbm_budget : c->budget;
+	memset(&S->stats, 0, sizeof(S->stats));
+	const size_t n = (size_t)S->cfg.max_inflight;
+	const size_t tab = (n * sizeof(MixedRender) + 255) / 256 * 256;
+	const size_t pre = (n * sizeof(unsigned long long) + 255) / 256 * 256;
+	const size_t cnt = 64 * GROUPS + 8 * GROUPS;
+	S->dbytes = tab + pre + cnt + 256;
+	int st = gi_dalloc(c, &S->dblock, S->dbytes);
+	cudaError_t e = cudaSuccess;
+	if(!st) {
+		S->d_tab = (MixedRender *)S->dblock;
+		S->d_pre = (unsigned long long *)((char *)S->dblock + tab);
+		S->d_queue = (unsigned int *)((char *)S->dblock + tab + pre);
+		S->d_steps = (unsigned long long *)((char *)S->dblock + tab + pre + 64 * GROUPS);
+		void *h = nullptr;
+		e = cudaMallocHost(&h, tab + pre + 8 * GROUPS);
+		if(e == cudaSuccess) {
+			S->h_tab = (MixedRender *)h;
+			S->h_pre = (unsigned long long *)((char *)h + tab);
+			S->h_steps = (unsigned long long *)((char *)h + tab + pre);
+		}
+		for(int i = 0; i < 2 && e == cudaSuccess; ++i)
+			e = cudaStreamCreateWithFlags(&S->s[i], cudaStreamNonBlocking);
+		if(e == cudaSuccess) e = cudaEventCreateWithFlags(&S->copied, cudaEventDisableTiming);
+		if(e == cudaSuccess) e = cudaEventCreate(&S->e0);
+		if(e == cudaSuccess) e = cudaEventCreate(&S->e1);
+		if(e == cudaSuccess) e = cudaEventCreateWithFlags(&S->e2, cudaEventDisableTiming);
+		if(e != cudaSuccess)
+			st = gi_from_cuda(e);
+	}
+	if(st) {
+		free_server(S);
+		return st;
+	}
+	c->server = S;
+	try {
+		S->th = std::thread(loop, S);
+	} catch(...) {
+		c->server = nullptr;
+		free_server(S);
+		return GRAY_ENOMEM;
+	}
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_serve_submit(gray_ctx *c, const gray_render_desc *d, uint64_t *id)
+{
+	if(!c || !c->server || !id)
+		return c && !c->server ? GRAY_ESTATE : GRAY_EINVAL;
+	int st = gray_internal_check_desc(d);
+	if(st)
+		return st;
+	if(d->precision != GRAY_PREC_MIXED)
+		return GRAY_EINVAL; /* the server runs the mixed-precision kernels */
+	if(d->spacetime == GRAY_ST_NUMERICAL && !gi_grid_ready(c))
+		return GRAY_ESTATE;
+	if(d->n_dump > (uint64_t)INT32_MAX)
+		return GRAY_EINVAL;
+	Request *r = new(std::nothrow) Request;
+	if(!r)
+		return GRAY_ENOMEM;
+	r->desc = *d;
+	gray_internal_make_params(d, &r->p);
+	r->bytes = (size_t)r->p.n_rays * (r->p.n_data + 1) * sizeof(double);
+	Server *S = c->server;
+	{
+		std::lock_guard<std::mutex> lk(S->mu);
+		if(S->stop) {
+			delete r;
+			return GRAY_ESTATE;
+		}
+		r->id = S->next_id++;
+		r->t_submit = now_s();
+		if(r->bytes > S->budget) { /* can never be admitted */
+			r->state = GRAY_REQ_FAILED;
+			r->status = GRAY_EBUDGET;
+			r->t_done = r->t_submit;
+			S->stats.failed++;
+		} else {
+			S->pending.push_back(r);
+		}
+		S->reqs[r->id] = r;
+		*id = r->id;
+	}
+	S->cv.notify_all();
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_serve_poll(gray_ctx *c, uint64_t id, gray_request_status *out)
+{
+	if(!c || !out)
+		return GRAY_EINVAL;
+	if(!c->server)
+		return GRAY_ESTATE;
+	Server *S = c->server;
+	std::lock_guard<std::mutex> lk(S->mu);
+	auto it = S->reqs.find(id);
+	if(it == S->reqs.end())
+		return GRAY_ENOTFOUND;
+	const Request *r = it->second;
+	out->state = r->state;
+	out->status = r->status;
+	out->t_submit = r->t_submit;
+	out->t_admit = r->t_admit;
+	out->t_done = r->t_done;
+	out->n_rays = (uint64_t)r->p.n_rays;
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_serve_result(gray_ctx *c, uint64_t id, void *data, size_t data_bytes, void *info,
+                  size_t info_bytes)
+{
+	if(!c)
+		return GRAY_EINVAL;
+	if(!c->server)
+		return GRAY_ESTATE;
+	Server *S = c->server;
+	std::lock_guard<std::mutex> lk(S->mu);
+	auto it = S->reqs.find(id);
+	if(it == S->reqs.end())
+		return GRAY_ENOTFOUND;
+	Request *r = it->second;
+	if(r->state == GRAY_REQ_QUEUED || r->state == GRAY_REQ_RUNNING)
+		return GRAY_ESTATE;
+	if(r->state == GRAY_REQ_DONE) {
+		if(data && data_bytes != r->h_data.size() * sizeof(double))
+			return GRAY_ESIZE;
+		if(info && info_bytes != r->h_info.size() * sizeof(double))
+			return GRAY_ESIZE;
+		if(data)
+			memcpy(data, r->h_data.data(), data_bytes);
+		if(info)
+			memcpy(info, r->h_info.data(), info_bytes);
+	}
+	int st = r->state == GRAY_REQ_DONE ? GRAY_OK
+	         : r->state == GRAY_REQ_FAILED ? (r->status ? r->status : GRAY_ECUDA)
+	                                        : GRAY_ESTATE;
+	S->reqs.erase(it);
+	delete r;
+	return st;
+}
+
+extern "C" int
+gray_serve_cancel(gray_ctx *c, uint64_t id)
+{
+	if(!c)
+		return GRAY_EINVAL;
+	if(!c->server)
+		return GRAY_ESTATE;
+	Server *S = c->server;
+	std::lock_guard<std::mutex> lk(S->mu);
+	auto it = S->reqs.find(id);
+	if(it == S->reqs.end())
+		return GRAY_ENOTFOUND;
+	it->second->cancel = true; /* retired at the next iteration boundary */
+	S->cv.notify_all();
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_serve_get_stats(gray_ctx *c, gray_serve_stats *out)
+{
+	if(!c || !out)
+		return GRAY_EINVAL;
+	if(!c->server)
+		return GRAY_ESTATE;
+	std::lock_guard<std::mutex> lk(c->server->mu);
+	*out = c->server->stats;
+	return c->server->thread_status;
+}
+
+extern "C" int
+gray_serve_stop(gray_ctx *c, int drain)
+{
+	if(!c)
+		return GRAY_EINVAL;
+	if(!c->server)
+		return GRAY_ESTATE;
+	Server *S = c->server;
+	{
+		std::lock_guard<std::mutex> lk(S->mu);
+		S->stop = true;
+		S->drain = drain != 0;
+	}
+	S->cv.notify_all();
+	if(S->th.joinable())
+		S->th.join();
+	int st = S->thread_status;
+	free_server(S);
+	c->server = nullptr;
+	return st;
+}

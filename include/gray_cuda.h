@@ -200,6 +200,60 @@ int gray_plan(gray_ctx *ctx, int batch_id, int flags, gray_launch_plan *best);
 int gray_set_plan(gray_ctx *ctx, const gray_launch_plan *plan);
 int gray_get_plan(const gray_ctx *ctx, gray_launch_plan *plan);
 
+/* ---- serving: continuous batching (no reference counterpart) -------- */
+
+/* A scheduler thread owned by the context admits submitted renders as HBM
+ * (the configured budget) and table slots free up, and advances every
+ * admitted render by dumps_per_iter dump intervals per iteration: one
+ * persistent launch per kind (analytic by n_freq, numerical), so renders
+ * that arrived while others run share the device with them.  Finished
+ * renders are copied to host memory and their device state is freed.  Only
+ * mixed-precision renders are served; numerical ones use the context's
+ * grid, which must be loaded before gray_serve_start.  While the server
+ * runs, only gray_serve_* may be called on the context (they are
+ * thread-safe). */
+enum gray_req_state {
+	GRAY_REQ_QUEUED    = 0,
+	GRAY_REQ_RUNNING   = 1,
+	GRAY_REQ_DONE      = 2,
+	GRAY_REQ_FAILED    = 3,
+	GRAY_REQ_CANCELLED = 4
+};
+
+typedef struct gray_serve_config {
+	size_t  hbm_budget;      /* bytes of admitted render state (0: the context's) */
+	int32_t max_inflight;    /* renders admitted at once (0: 1024)              */
+	int32_t dumps_per_iter;  /* dump intervals per iteration (0: 1)             */
+} gray_serve_config;
+
+typedef struct gray_request_status {
+	int32_t  state;          /* enum gray_req_state                        */
+	int32_t  status;         /* GRAY_E* of a failed request                */
+	double   t_submit;       /* gray_serve_clock() seconds                 */
+	double   t_admit;
+	double   t_done;
+	uint64_t n_rays;
+} gray_request_status;
+
+typedef struct gray_serve_stats {
+	uint64_t iterations;
+	uint64_t ray_steps[2];   /* [0] analytic, [1] numerical                */
+	uint64_t completed, failed, cancelled;
+	double   busy_s;         /* device time of the iterations (events)    */
+} gray_serve_stats;
+
+double gray_serve_clock(void);
+int gray_serve_start(gray_ctx *ctx, const gray_serve_config *cfg);
+int gray_serve_submit(gray_ctx *ctx, const gray_render_desc *desc, uint64_t *request_id);
+int gray_serve_poll(gray_ctx *ctx, uint64_t request_id, gray_request_status *out);
+/* Copy a finished request's state (SoA, as gray_read_state) and release it. */
+int gray_serve_result(gray_ctx *ctx, uint64_t request_id, void *data, size_t data_bytes,
+                      void *info, size_t info_bytes);
+int gray_serve_cancel(gray_ctx *ctx, uint64_t request_id);
+int gray_serve_get_stats(gray_ctx *ctx, gray_serve_stats *out);
+/* drain != 0: finish every submitted request first; else drop them. */
+int gray_serve_stop(gray_ctx *ctx, int drain);
+
 /* ---- numerical spacetime (sim-org/io.c:302-533, interp.cl, dyst.cl) - */
 
 typedef struct gray_grid_desc {
