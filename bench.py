@@ -45,7 +45,8 @@ from gray_b200 import configs, flops  # noqa: E402
 
 WORKLOADS = {"torus_rt_1024": configs.TORUS_RT_1024,
              "kerr_small_64": configs.KERR_SMALL_64,
-             "survey_256": None}  # a batch of 256 renders (configs.survey)
+             "survey_256": None,  # a batch of 256 renders (configs.survey)
+             "serve_mix": None}   # Poisson request stream (configs.serve_requests)
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 METRIC = "ray-steps/s"
 
@@ -75,6 +76,14 @@ def parse():
                     help="launch shape of the persistent kernel (measure = autotune)")
     ap.add_argument("--fp64-renders", type=int, default=16,
                     help="survey_256: renders run one at a time in FP64 for the comparison")
+    ap.add_argument("--rates", default="1,2,3,4,6,8,12",
+                    help="serve_mix: arrival rates (requests/s) swept in order")
+    ap.add_argument("--requests", type=int, default=32, help="serve_mix: requests per rate")
+    ap.add_argument("--partition", default="replicate", choices=["replicate", "split"],
+                    help="survey_256 on N GPUs: every rank renders the survey (weak) or "
+                         "the renders are split across ranks (strong)")
+    ap.add_argument("--dumps-per-iter", type=int, default=4,
+                    help="serve_mix: dump intervals each server iteration advances")
     return ap.parse_args()
 
 
@@ -209,9 +218,11 @@ def timed_renders(torch, render, k, flush):
 
 
 def max_over_ranks(torch, dist, x):
+    """The slowest rank's time: the only collective of a multi-GPU run."""
     if dist is None:
         return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cpu" if dist.get_backend() == "gloo" else "cuda"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -384,6 +395,12 @@ def survey_arm(args, rank, local_rank, world, dist):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     peak32 = ctx.measure_peak(api.PREC_MIXED)
     cfgs = configs.survey()
+    scaling = "weak"
+    if args.partition == "split" and world > 1:
+        # strong scaling: the 256 renders are split across the ranks
+        from gray_b200 import shard
+        cfgs = shard.my_share(cfgs, [c["n_width"] * c["n_height"] for c in cfgs], rank, world)
+        scaling = "strong"
     nf = len(cfgs[0]["nu"])
     rs = [ctx.render(dict(c, precision=api.PREC_MIXED)) for c in cfgs]
     n_rays = sum(r.n_rays for r in rs)
@@ -481,7 +498,7 @@ def survey_arm(args, rank, local_rank, world, dist):
     line = {
         "metric": METRIC, "value": value, "unit": "ray-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "higher_is_better": True, "scaling": scaling, "vs_baseline": None,
         "dtype": "f32+f64-islands", "data": "synthetic",
         "config": {"workload": "survey_256", "renders": len(cfgs), "rays_per_step": n_rays,
                    "seed": configs.SURVEY_SEED, "n_freq": nf, "ray_steps_per_step": steps,
@@ -494,11 +511,136 @@ def survey_arm(args, rank, local_rank, world, dist):
     print(json.dumps(line), flush=True)
 
 
+def serve_arm(args, rank, local_rank, world, dist):
+    """serve_mix: seeded Poisson arrivals of analytic (70%) and numerical
+    (30%) render requests into the continuous-batching server, with a
+    device-resident 256^3 grid and a 120 GB admission budget; the arrival
+    rate is swept upward until p99 latency exceeds 4 x p50."""
+    import time
+    import torch
+    from gray_b200 import api
+
+    torch.cuda.set_device(local_rank)
+    ctx = api.Context(local_rank)
+    n = configs.SERVE_GRID_N
+    grid = api.make_grid(n, -configs.SERVE_GRID_BOX, configs.SERVE_GRID_BOX, 0.0, 0.0, physics=True)
+    ctx.make_boosted_ks(grid, 0.7, 0.3, 1, 0.0, 0)
+    rates = [float(x) for x in args.rates.split(",")]
+    # the same seeded request set at every rate, so the points compare
+    reqs = configs.serve_requests(args.requests) * len(rates)
+    rng = np.random.Generator(np.random.PCG64(configs.SERVE_SEED + 1))
+    budget = int(120e9)
+    ctx.serve_start(hbm_budget=budget, max_inflight=256, dumps_per_iter=args.dumps_per_iter)
+    sweep, sustained, k0 = [], None, 0
+    sample = {}  # class -> (cfg, served state) for the FP64 comparison
+    try:
+        # warm-up: one request of each kind
+        first = {}
+        for c in configs.serve_requests(32, seed=configs.SERVE_SEED + 2):
+            first.setdefault(c.get("spacetime", 0), configs.scaled(c, 64))
+        w = [ctx.submit(c) for c in first.values()]
+        while any(ctx.poll(i).state < api.REQ_DONE for i in w):
+            time.sleep(0.005)
+        for i in w:
+            ctx.release(i)
+        for rate in rates:
+            batch = reqs[k0:k0 + args.requests]
+            k0 += args.requests
+            gaps = rng.exponential(1.0 / rate, len(batch))
+            s0, _ = ctx.serve_stats()
+            steps0 = sum(s0.ray_steps)
+            t_start = ctx.clock()
+            due = t_start + np.cumsum(gaps)
+            ids, pending = [], list(range(len(batch)))
+            while pending:
+                now = ctx.clock()
+                if due[pending[0]] <= now:
+                    j = pending.pop(0)
+                    ids.append((ctx.submit(batch[j]), j))
+                else:
+                    time.sleep(min(0.002, due[pending[0]] - now))
+            lat, kinds, t_end = [], [], t_start
+            for rid, j in ids:
+                while ctx.poll(rid).state < api.REQ_DONE:
+                    time.sleep(0.002)
+                s = ctx.poll(rid)
+                lat.append(s.t_done - s.t_submit)
+                t_end = max(t_end, s.t_done)
+                kind = "numerical" if batch[j].get("spacetime") == 1 else "analytic"
+                kinds.append(kind)
+                if kind not in sample and batch[j]["n_width"] <= 256:
+                    nd = 8 + 2 * len(batch[j]["nu"])
+                    sample[kind] = (batch[j], ctx.result(rid, nd, s.n_rays)[0])
+                else:
+                    ctx.release(rid)
+            s1, st = ctx.serve_stats()
+            steps = sum(s1.ray_steps) - steps0
+            lat = np.array(lat)
+            p50, p99 = float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
+            row = {"rate_per_s": rate, "requests": len(batch), "p50_s": p50, "p99_s": p99,
+                   "throughput": steps / (t_end - t_start), "wall_s": t_end - t_start,
+                   "p50_by_class": {k: float(np.percentile(lat[np.array(kinds) == k], 50))
+                                     for k in set(kinds)}}
+            sweep.append(row)
+            if p99 > 4 * p50:
+                break
+            sustained = row
+        stats, _ = ctx.serve_stats()
+    finally:
+        ctx.serve_stop()
+    # mixed-vs-FP64 error per class on one sampled request each
+    errs = {}
+    for kind, (cfg, got) in sample.items():
+        r = ctx.render(dict(cfg, precision=api.PREC_FP64))
+        r.run()
+        ref = r.state(api.LAYOUT_SOA)[0]
+        r.close()
+        if kind == "analytic":
+            errs[kind] = {"image_rel_l2_err": max(float(np.linalg.norm(got[8 + i] - ref[8 + i]) /
+                                                        np.linalg.norm(ref[8 + i])) for i in range(4))}
+        else:
+            # the numerical spacetime has no horizon stop (dyst.cl:43-53 gives
+            # eps = 1), so captured rays run on inside the singular region where
+            # FP32 and FP64 part ways; the image is the escaping rays (end
+            # radius above 100 M in FP64)
+            fin = np.all(np.isfinite(ref), axis=0) & np.all(np.isfinite(got), axis=0)
+            esc = fin & (np.sqrt(np.sum(ref[1:4] ** 2, axis=0)) > 100.0)
+            errs[kind] = {"end_position_rel_l2_err_escaping": float(
+                np.linalg.norm(got[1:4, esc] - ref[1:4, esc]) / np.linalg.norm(ref[1:4, esc])),
+                "escaping_fraction": float(esc.mean())}
+        errs[kind]["rays"] = int(ref.shape[1])
+    ctx.close()
+    if rank != 0:
+        return
+    best = sustained or sweep[0]
+    line = {
+        "metric": METRIC, "value": best["throughput"], "unit": "ray-steps/s", "n_gpus": world,
+        "steps": len(sweep), "warmup": 1, "ms_per_step": 1e3 * best["wall_s"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64-islands", "data": "synthetic",
+        "config": {"workload": "serve_mix", "requests_per_rate": args.requests,
+                   "grid": "%d^3 FP32 boosted KS (a=0.7, v=0.3 along x), %.2f GB" %
+                           (n, n ** 3 * 52 * 4 / 1e9),
+                   "hbm_budget_bytes": budget, "dumps_per_iter": args.dumps_per_iter,
+                   "mix": "70% analytic torus 64..1024^2, 30% numerical 64..512^2"},
+        "latency": {"p50_s": best["p50_s"], "p99_s": best["p99_s"],
+                    "sustained_rate_per_s": best["rate_per_s"]},
+        "sweep": sweep, "error_vs_fp64": errs,
+        "serve_stats": {"iterations": stats.iterations, "busy_s": stats.busy_s,
+                        "completed": stats.completed},
+        "e2e": {"value": best["throughput"], "unit": "ray-steps/s",
+                "note": "request submit to result in host memory, host clock"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.workload == "survey_256":
         # the reference arm samples the survey's median-index render
         cfg = configs.survey()[128]
+    elif args.workload == "serve_mix":
+        cfg = configs.serve_requests(8)[0]  # an analytic request of the stream
     else:
         cfg = dict(WORKLOADS[args.workload])
     if args.side:
@@ -521,6 +663,8 @@ def main():
     try:
         if args.workload == "survey_256":
             survey_arm(args, rank, local_rank, world, dist)
+        elif args.workload == "serve_mix":
+            serve_arm(args, rank, local_rank, world, dist)
         else:
             ours_arm(args, cfg, rank, local_rank, world, dist)
     finally:

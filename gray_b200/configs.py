@@ -49,6 +49,37 @@ def survey(n=256, seed=SURVEY_SEED, side_lo=32, side_hi=512):
     return out
 
 
+SERVE_SEED = 20261204
+SERVE_GRID_N = 256          # 256^3 FP32 boosted KS, one time level: 3.5 GB resident
+SERVE_GRID_BOX = 40.0
+NUMERICAL_BASE = dict(       # numerical-spacetime camera of the serving mix
+    a_spin=0.0, r_obs=200.0, w_img=80.0, h_img=80.0, j_obs=0.0, t_init=0.0,
+    dt_dump=-10.0, n_dump=30, n_sub=100, nu=(), spacetime=1)
+
+
+def serve_requests(n, seed=SERVE_SEED):
+    """serve_mix request stream: 70% analytic torus renders (side log-uniform
+    64..1024, spin U[0, 0.998], inclination U[5, 85] deg, camera at 1000 M)
+    and 30% numerical-spacetime renders on the shared boosted-KS grid (side
+    log-uniform 64..512, inclination U[5, 85] deg, camera at 200 M, affine
+    range -300 M in steps of 0.01 M)."""
+    import numpy as np
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for _ in range(n):
+        numerical = rng.uniform() < 0.3
+        inc = float(rng.uniform(5.0, 85.0))
+        if numerical:
+            side = int(np.rint(np.exp(rng.uniform(np.log(64), np.log(512)))))
+            c = dict(NUMERICAL_BASE, i_obs=inc, n_width=side, n_height=side)
+        else:
+            side = int(np.rint(np.exp(rng.uniform(np.log(64), np.log(1024)))))
+            c = dict(TORUS_RT_1024, a_spin=float(rng.uniform(0.0, 0.998)), i_obs=inc,
+                     n_width=side, n_height=side)
+        out.append(c)
+    return out
+
+
 def scaled(cfg, side):
     """The same workload on a side x side camera (parity-test sizes)."""
     c = dict(cfg)
