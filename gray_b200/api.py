@@ -29,6 +29,7 @@ EXPORTS = [
     "gray_set_stream", "gray_sync", "gray_hbm_used", "gray_render_create",
     "gray_render_destroy", "gray_icond", "gray_evolve", "gray_run", "gray_evolve_all",
     "gray_read_state", "gray_write_state", "gray_read_kdown", "gray_ray_steps",
+    "gray_gather_steps",
     "gray_load_spacetime", "gray_load_spacetime_interleaved",
     "gray_make_boosted_ks", "gray_swap_levels", "gray_measure_peak",
     "gray_run_mixed_noalloc", "gray_read_spacetime",
@@ -163,6 +164,7 @@ def lib():
         L.gray_write_state.argtypes = [vp, i, vp, sz, i]
         L.gray_read_kdown.argtypes = [vp, i, vp, sz]
         L.gray_ray_steps.argtypes = [vp, i, P(u64)]
+        L.gray_gather_steps.argtypes = [vp, i, P(u64)]
         L.gray_load_spacetime.argtypes = [vp, P(GridDesc), P(ctypes.c_void_p), i]
         L.gray_load_spacetime_interleaved.argtypes = [vp, P(GridDesc), vp, i]
         L.gray_make_boosted_ks.argtypes = [vp, P(GridDesc), d, d, i, d, i]
@@ -269,6 +271,11 @@ class Render:
     def steps(self):
         v = ctypes.c_uint64(0)
         _ck(lib().gray_ray_steps(self.ctx.h, self.id, ctypes.byref(v)), "gray_ray_steps")
+        return v.value
+
+    def gather_steps(self):
+        v = ctypes.c_uint64(0)
+        _ck(lib().gray_gather_steps(self.ctx.h, self.id, ctypes.byref(v)), "gray_gather_steps")
         return v.value
 
     def close(self):

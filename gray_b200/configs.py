@@ -49,6 +49,12 @@ def survey(n=256, seed=SURVEY_SEED, side_lo=32, side_hi=512):
     return out
 
 
+NUMERICAL_128 = dict(        # 128^3 grid, two levels, 512^2 camera at 200 M, 45 deg
+    a_spin=0.0, r_obs=200.0, i_obs=45.0, j_obs=0.0, w_img=80.0, h_img=80.0,
+    n_width=512, n_height=512, t_init=0.0, dt_dump=-10.0, n_dump=30, n_sub=100,
+    nu=(), spacetime=1)
+NUMERICAL_GRID = dict(n=128, box=40.0, a=0.7, v=0.3, axis=1, t1=0.0, t2=10.0)
+
 SERVE_SEED = 20261204
 SERVE_GRID_N = 256          # 256^3 FP32 boosted KS, one time level: 3.5 GB resident
 SERVE_GRID_BOX = 40.0

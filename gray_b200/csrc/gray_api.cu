@@ -426,7 +426,7 @@ gray_render_destroy(gray_ctx *c, int id)
 static int
 icond_impl(gray_ctx *c, Render *r)
 {
-	CK(cudaMemsetAsync(r->d_steps, 0, sizeof(unsigned long long), c->stream));
+	CK(cudaMemsetAsync(r->d_steps, 0, 2 * sizeof(unsigned long long), c->stream));
 	if(r->p.spacetime == GRAY_ST_NUMERICAL) {
 		if(!grid_ready(c))
 			return GRAY_ESTATE;
@@ -467,7 +467,7 @@ run_mixed(gray_ctx *c, Render *r, double t_init, double dt_dump, long long n_dum
 		if(!grid_ready(c))
 			return GRAY_ESTATE;
 		CK(launch_dyst_mixed_table(T, c->grid->gp, r->d_queue, r->d_steps, c->stream,
-		                           c->mixed));
+		                           c->mixed, r->d_steps + 1));
 	} else {
 		CK(launch_mixed_table(T, r->p.n_freq, r->d_queue, r->d_steps, c->stream, c->mixed));
 	}
@@ -649,7 +649,7 @@ gray_write_state(gray_ctx *c, int id, const void *data, size_t data_bytes, int l
 	}
 	if(r->p.spacetime == GRAY_ST_KERR)
 		CK(launch_getuu64(r->p, r->d_data, r->d_info, c->stream));
-	CK(cudaMemsetAsync(r->d_steps, 0, sizeof(unsigned long long), c->stream));
+	CK(cudaMemsetAsync(r->d_steps, 0, 2 * sizeof(unsigned long long), c->stream));
 	CK(cudaStreamSynchronize(c->stream));
 	r->has_state = true;
 	return GRAY_OK;
@@ -1226,5 +1226,21 @@ gray_plan(gray_ctx *c, int id, int flags, gray_launch_plan *best)
 	c->mixed = best_cfg;
 	gray_get_plan(c, best);
 	best->ns = best_ns;
+	return GRAY_OK;
+}
+
+extern "C" int
+gray_gather_steps(gray_ctx *c, int id, uint64_t *steps)
+{
+	Render *r = find(c, id);
+	if(!r)
+		return GRAY_ENOTFOUND;
+	if(!steps)
+		return GRAY_EINVAL;
+	CK(cudaSetDevice(c->device));
+	unsigned long long v = 0;
+	CK(cudaMemcpyAsync(&v, r->d_steps + 1, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
+	CK(cudaStreamSynchronize(c->stream));
+	*steps = v;
 	return GRAY_OK;
 }

@@ -125,11 +125,27 @@ dyst_rhs32(const GridParams &g, const DystConst &dc, const float *s, float *ds)
 		if(g.physics)
 			ft = fminf(fmaxf(ft, 0.0f), 1.0f);
 	}
-	float2 acc[20];
+	/* u^a u^b over the 10 stored (a <= b) components, off-diagonal doubled */
+	float p[10];
+	{
+		int k = 0;
 #pragma unroll
-	for(int k = 0; k < 20; ++k)
-		acc[k] = make_float2(0.0f, 0.0f);
+		for(int i = 0; i < 4; ++i)
+#pragma unroll
+			for(int j = i; j < 4; ++j) {
+				float uu = u[i] * u[j];
+				p[k++] = i == j ? uu : 2.0f * uu;
+			}
+	}
+	/* Interpolation and the contraction with u u are both linear, so each
+	 * corner's 40 Gamma are contracted first (4 sums) and only the sums are
+	 * weighted: 4 accumulators instead of 40 keeps registers for warps. */
+	float Gm[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 	const float ax = 1.0f - w[0], ay = 1.0f - w[1], az = 1.0f - w[2];
+	/* a time level whose weight is zero (t outside [t1, t2] in physics
+	 * mode, where the factor is clamped) is not fetched at all */
+	const bool use0 = g.single || ft < 1.0f;
+	const bool use1 = !g.single && ft > 0.0f;
 #pragma unroll
 	for(int c = 0; c < 8; ++c) {
 		float wc = ((c & 1) ? w[0] : ax) * ((c & 2) ? w[1] : ay) * ((c & 4) ? w[2] : az);
@@ -137,37 +153,26 @@ dyst_rhs32(const GridParams &g, const DystConst &dc, const float *s, float *ds)
 		int iy = (c & 2) ? i1[1] : i0[1];
 		int iz = (c & 4) ? i1[2] : i0[2];
 		long long row = (((long long)iz * g.ny + iy) * g.nx + ix) * GRAY_NSTRIDE;
-		const int nl = g.single ? 1 : 2;
-		for(int l = 0; l < nl; ++l) {
+		for(int l = 0; l < 2; ++l) {
+			if(!(l ? use1 : use0))
+				continue;
 			float wl = g.single ? wc : wc * (l ? ft : 1.0f - ft);
-			const float2 W = make_float2(wl, wl);
 			const float4 *src = (const float4 *)(g.lvl[l] + row);
+			float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
 			for(int k = 0; k < 10; ++k) {
 				float4 v = __ldg(src + k);
-				acc[2 * k]     = __ffma2_rn(W, make_float2(v.x, v.y), acc[2 * k]);
-				acc[2 * k + 1] = __ffma2_rn(W, make_float2(v.z, v.w), acc[2 * k + 1]);
+				const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+				for(int q = 0; q < 4; ++q) {
+					const int idx = 4 * k + q; /* Gamma^(idx/10)_(idx%10) */
+					s[idx / 10] = fmaf(e[q], p[idx % 10], s[idx / 10]);
+				}
 			}
+#pragma unroll
+			for(int m = 0; m < 4; ++m)
+				Gm[m] = fmaf(wl, s[m], Gm[m]);
 		}
-	}
-	const float *G = (const float *)acc; /* Gamma 0..39 */
-	float p[10];
-	int k = 0;
-#pragma unroll
-	for(int i = 0; i < 4; ++i)
-#pragma unroll
-		for(int j = i; j < 4; ++j) {
-			float uu = u[i] * u[j];
-			p[k++] = i == j ? uu : 2.0f * uu;
-		}
-	float Gm[4];
-#pragma unroll
-	for(int m = 0; m < 4; ++m) {
-		float a = G[10 * m] * p[0];
-#pragma unroll
-		for(int kk = 1; kk < 10; ++kk)
-			a = fmaf(G[10 * m + kk], p[kk], a);
-		Gm[m] = a;
 	}
 #pragma unroll
 	for(int m = 0; m < 4; ++m)
@@ -176,7 +181,8 @@ dyst_rhs32(const GridParams &g, const DystConst &dc, const float *s, float *ds)
 
 __global__ void __launch_bounds__(256, 2)
 dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
-                  unsigned int *__restrict__ queue, unsigned long long *__restrict__ steps)
+                  unsigned int *__restrict__ queue, unsigned long long *__restrict__ steps,
+                  unsigned long long *__restrict__ inbox)
 {
 	constexpr int ND = 8;
 	const unsigned FULL = 0xffffffffu;
@@ -186,7 +192,7 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 	int dump = 0, h = 0, dh_step = 0, n = 0;
 	float dtn = 0.0f;
 	bool active = false, exhausted = false;
-	unsigned long long cnt = 0;
+	unsigned long long cnt = 0, cnt_in = 0; /* all steps; steps that interpolate */
 	const MixedRender *c = nullptr;
 
 	for(;;) {
@@ -252,6 +258,7 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 		int dh = dh_step < n - h ? dh_step : n - h;
 		const float hs = (float)dh * dtn, hh = 0.5f * hs;
 		float k[ND], t[ND], sum[ND];
+		cnt_in += (!g.physics || inside32(g, hi)) ? 1 : 0;
 		dyst_rhs32(g, dc, hi, k);
 #pragma unroll
 		for(int i = 0; i < ND; ++i) {
@@ -296,10 +303,14 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 		}
 	}
 #pragma unroll
-	for(int o = 16; o > 0; o >>= 1)
+	for(int o = 16; o > 0; o >>= 1) {
 		cnt += __shfl_xor_sync(FULL, cnt, o);
+		cnt_in += __shfl_xor_sync(FULL, cnt_in, o);
+	}
 	if(lane == 0 && cnt)
 		atomicAdd(steps, cnt);
+	if(lane == 0 && cnt_in && inbox)
+		atomicAdd(inbox, cnt_in);
 }
 
 [[maybe_unused]] inline unsigned
@@ -312,7 +323,8 @@ blocks_for(long long n, int block)
 
 cudaError_t
 launch_dyst_mixed_table(const MixedTable &T, const GridParams &g, unsigned int *queue,
-                        unsigned long long *steps, cudaStream_t st, const MixedLaunch &cfg)
+                        unsigned long long *steps, cudaStream_t st, const MixedLaunch &cfg,
+                        unsigned long long *inbox)
 {
 	DystConst dc;
 	for(int a = 0; a < 3; ++a) {
@@ -336,7 +348,7 @@ launch_dyst_mixed_table(const MixedTable &T, const GridParams &g, unsigned int *
 	unsigned grid = (unsigned)(want < need ? want : need);
 	if(grid == 0)
 		grid = 1;
-	dyst_mixed_kernel<<<grid, block, 0, st>>>(T, g, dc, queue, steps);
+	dyst_mixed_kernel<<<grid, block, 0, st>>>(T, g, dc, queue, steps, inbox);
 	return cudaGetLastError();
 }
 

@@ -41,10 +41,12 @@ cudaError_t launch_mixed_table(const MixedTable &T, int n_freq, unsigned int *qu
                                unsigned long long *steps, cudaStream_t st,
                                const MixedLaunch &cfg);
 
-/* numerical spacetime: every render of the table on the same grid */
+/* numerical spacetime: every render of the table on the same grid; inbox
+ * (nullable) accumulates the steps that interpolate the grid */
 cudaError_t launch_dyst_mixed_table(const MixedTable &T, const GridParams &g,
                                     unsigned int *queue, unsigned long long *steps,
-                                    cudaStream_t st, const MixedLaunch &cfg);
+                                    cudaStream_t st, const MixedLaunch &cfg,
+                                    unsigned long long *inbox = nullptr);
 
 /* resident blocks per SM of the mixed kernel for a launch shape */
 cudaError_t mixed_occupancy(int n_freq, const MixedLaunch &cfg, int *blocks_per_sm);

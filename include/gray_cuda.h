@@ -163,6 +163,10 @@ int gray_read_kdown(gray_ctx *ctx, int render_id, double *k, size_t bytes);
 /* Accepted RK4 steps summed over the render's rays since the last icond. */
 int gray_ray_steps(gray_ctx *ctx, int render_id, uint64_t *steps);
 
+/* Of those, the steps that interpolated the numerical grid (mixed
+ * numerical renders; in physics mode steps outside the box do not). */
+int gray_gather_steps(gray_ctx *ctx, int render_id, uint64_t *steps);
+
 /* ---- batches, launch plans, graphs ---------------------------------- */
 
 /* A batch is many mixed-precision renders integrated by ONE persistent
