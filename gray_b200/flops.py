@@ -7,11 +7,13 @@ and copies are free.  Counts assume the ray is inside the emission region
 every step of the torus workloads; outside it the transfer part is skipped.
 
 Mixed kernel (gray_b200/csrc/kernels_mixed.cu), per call:
-  ks_rhs32        197  (head 42: radius root, f and its gradient with
-                        2 rsqrt + 2 rcp; l and its gradient 33; D tensors,
-                        contractions and the acceleration 122)
-  torus_rt32      46 + 6 per frequency  (Keplerian flow 34, density 8 with
-                        1 ex2, shift^-0.7 with lg2 + ex2, 1 ex2 per frequency)
+  ks_rhs          166  (head 42: radius root, f and its gradient with
+                        2 rsqrt + 2 rcp; l and its gradient 33; the two
+                        contractions of d(f l.u l) taken directly, without
+                        the nine D_a^i, and the acceleration 91)
+  torus_rt        47 + 5 per frequency  (Keplerian flow 34, density 8 with
+                        1 ex2, j/shift^2 with lg2 + ex2 factored once, 1 ex2
+                        per frequency)
   RK4 + Kahan     per component: stages 2 + 4 + 4, final 2 + 4 (Kahan)
                   = 16, plus 3 scalars
   step control    17  (FP32 radius root and the n/|dt| tick rule)
@@ -29,7 +31,7 @@ The reference's own comments count the same KS RHS as about 205 FLOP
 
 def mixed_per_step(n_freq, transfer=True):
     nd = 8 + 2 * n_freq
-    rhs = 197 + ((46 + 6 * n_freq) if (transfer and n_freq) else 0)
+    rhs = 166 + ((47 + 5 * n_freq) if (transfer and n_freq) else 0)
     return 4 * rhs + 16 * nd + 3 + 17
 
 
