@@ -14,12 +14,13 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libgray_cuda.so")
 MAX_FREQ = 8
+ABI_VERSION = 2  # GRAY_ABI_VERSION of include/gray_cuda.h
 
 OK, EINVAL, ENOMEM, ECUDA, ENODEV, EBUDGET, ETIMEOUT, ENOTFOUND, ESTATE, ESIZE = (
     0, -1, -2, -3, -4, -5, -6, -7, -8, -9)
 PREC_FP64, PREC_MIXED = 0, 1
 ST_KERR, ST_NUMERICAL = 0, 1
-FLOW_NONE, FLOW_TORUS = 0, 1
+FLOW_NONE, FLOW_TORUS, FLOW_THERMAL = 0, 1, 2
 TERM_EPS, TERM_RPLUS = 0, 1
 LAYOUT_SOA, LAYOUT_AOS = 0, 1
 
@@ -64,6 +65,8 @@ class RenderDesc(ctypes.Structure):
         ("torus_n0", ctypes.c_double), ("torus_kappa", ctypes.c_double),
         ("torus_hr", ctypes.c_double),
         ("spacetime", ctypes.c_int32), ("precision", ctypes.c_int32),
+        ("m_adm", ctypes.c_double), ("flow_te", ctypes.c_double),
+        ("flow_b", ctypes.c_double),
     ]
 
 
@@ -102,12 +105,13 @@ class GridDesc(ctypes.Structure):
 
 
 # Reference defaults (sim/gray.opts, sim/Kerr.opts, sim/infcam.opts,
-# sim-org/setup.opts).
+# sim-org/setup.opts, sim-org/param.opts M_ADM; flow.cl:51-52 te and b).
 DEFAULTS = dict(m_bh=4e6, a_spin=0.0, w_img=64.0, h_img=64.0, r_obs=1024.0,
                 i_obs=60.0, j_obs=0.0, n_width=512, n_height=512, t_init=0.0,
                 dt_dump=-32.0, n_sub=1024, n_dump=64, term=TERM_EPS, nu=(),
                 flow=None, torus_n0=1.0, torus_kappa=1.0, torus_hr=0.3,
-                spacetime=ST_KERR, precision=PREC_FP64)
+                spacetime=ST_KERR, precision=PREC_FP64, m_adm=4.3e6,
+                flow_te=1e12, flow_b=0.0)
 
 
 def make_desc(cfg):
@@ -115,7 +119,8 @@ def make_desc(cfg):
     c.update(cfg)
     d = RenderDesc()
     for k in ("m_bh", "a_spin", "w_img", "h_img", "r_obs", "i_obs", "j_obs",
-              "t_init", "dt_dump", "torus_n0", "torus_kappa", "torus_hr"):
+              "t_init", "dt_dump", "torus_n0", "torus_kappa", "torus_hr",
+              "m_adm", "flow_te", "flow_b"):
         setattr(d, k, float(c[k]))
     for k in ("n_width", "n_height", "n_sub", "n_dump", "term", "spacetime", "precision"):
         setattr(d, k, int(c[k]))
@@ -126,7 +131,10 @@ def make_desc(cfg):
     for i, v in enumerate(nu):
         d.nu[i] = float(v)
     flow = c["flow"]
-    d.flow = int(flow) if flow is not None else (FLOW_TORUS if nu else FLOW_NONE)
+    if flow is None:  # the transfer model each spacetime carries
+        flow = (FLOW_NONE if not nu else
+                FLOW_THERMAL if d.spacetime == ST_NUMERICAL else FLOW_TORUS)
+    d.flow = int(flow)
     return d
 
 
@@ -188,6 +196,9 @@ def lib():
         L.gray_serve_cancel.argtypes = [vp, u64]
         L.gray_serve_get_stats.argtypes = [vp, P(ServeStats)]
         L.gray_serve_stop.argtypes = [vp, i]
+        if L.gray_abi_version() != ABI_VERSION:
+            raise RuntimeError("libgray_cuda.so has ABI %d, this module expects %d; rebuild"
+                               % (L.gray_abi_version(), ABI_VERSION))
         _lib = L
     return _lib
 

@@ -29,6 +29,8 @@ struct Grid {
 	gray_grid_desc desc;
 	bool loaded[2] = {false, false};
 	float *lvl[2] = {nullptr, nullptr};
+	float *spare = nullptr;         /* third level of a snapshot series    */
+	float *staging = nullptr;       /* pinned host snapshot (series loads) */
 	double *nodes[3] = {nullptr, nullptr, nullptr};
 	float *nodes_f[3] = {nullptr, nullptr, nullptr};
 	size_t bytes = 0;
@@ -81,6 +83,13 @@ int  gi_from_cuda(cudaError_t e);
 int  gi_dalloc(gray_ctx *c, void **p, size_t bytes);
 void gi_dfree(gray_ctx *c, void *p, size_t bytes);
 int  gi_grid_ready(gray_ctx *c);
+Render *gi_find_render(gray_ctx *c, int id);
+int  gi_icond(gray_ctx *c, Render *r);
+int  gi_evolve_interval(gray_ctx *c, Render *r, double t, double target, uint64_t n_sub);
+int  gi_check_grid(const gray_grid_desc *g);
+int  gi_ensure_grid(gray_ctx *c, const gray_grid_desc *g);
+int  gi_timed_begin(gray_ctx *c);
+int  gi_timed_end(gray_ctx *c, double *ns);
 void gi_serve_shutdown(gray_ctx *c); /* serve.cu: stop and free the server */
 
 #endif /* GRAY_CTX_INTERNAL_H */

@@ -8,6 +8,7 @@
 #define GRAY_DYST64_CUH
 
 #include "gray_internal.h"
+#include "thermal.cuh"
 
 namespace dyst64 {
 
@@ -198,6 +199,87 @@ rk4_dyst64(const GridParams &g, double *s, double dt)
 	double h6 = dt / 6.0;
 #pragma unroll
 	for(int i = 0; i < 8; ++i)
+		s[i] = fma(h6, fma(2.0, k2[i] + k3[i], k1[i]) + k4[i], s[i]);
+}
+
+/* phys.cl:66-74 on the numerical spacetime with the thermal transfer of
+ * NF frequencies: the geodesic of dyst_rhs64, k = down(q, u) of
+ * dyst_down64 and n_e = rho from one cell search for all 51 fields (the
+ * reference interpolates field by field: same values).  In physics mode
+ * outside the box the spacetime is flat and n_e = 0. */
+template <int NF>
+__device__ __forceinline__ void
+dyst_rhs_rt64(const thermal::Flow &f, const GridParams &g, const double *s, double *ds)
+{
+	const double *u = s + 4;
+	double k[4], ne;
+	ds[0] = u[0]; ds[1] = u[1]; ds[2] = u[2]; ds[3] = u[3];
+	if(g.physics && !inside64(g, s)) {
+		ds[4] = ds[5] = ds[6] = ds[7] = 0.0;
+		k[0] = -u[0]; k[1] = u[1]; k[2] = u[2]; k[3] = u[3];
+		ne = 0.0;
+	} else {
+		double v[GRAY_NCOMP], p[10], G[4], M[4][4];
+		interp64(g, s, 0, GRAY_NCOMP, v);
+		int n = 0;
+#pragma unroll
+		for(int i = 0; i < 4; ++i)
+#pragma unroll
+			for(int j = i; j < 4; ++j) {
+				double uu = u[i] * u[j];
+				p[n++] = i == j ? uu : 2.0 * uu;
+			}
+#pragma unroll
+		for(int m = 0; m < 4; ++m) {
+			double acc = v[10 * m] * p[0];
+#pragma unroll
+			for(int kk = 1; kk < 10; ++kk)
+				acc = fma(v[10 * m + kk], p[kk], acc);
+			G[m] = acc;
+		}
+#pragma unroll
+		for(int m = 0; m < 4; ++m)
+			ds[4 + m] = fma(G[0], u[m], -G[m]);
+		if(g.bug_gzz)
+			v[49] = v[48];
+		n = 40;
+#pragma unroll
+		for(int i = 0; i < 4; ++i)
+#pragma unroll
+			for(int j = i; j < 4; ++j) {
+				M[i][j] = v[n];
+				M[j][i] = v[n];
+				++n;
+			}
+#pragma unroll
+		for(int i = 0; i < 4; ++i)
+			k[i] = fma(M[i][3], u[3], fma(M[i][2], u[2], fma(M[i][1], u[1], M[i][0] * u[0])));
+		ne = v[50];
+	}
+	thermal::rt_rhs<NF>(f, k, ne, s + 8 + NF, ds + 8, ds + 8 + NF);
+}
+
+/* RK4 of the geodesic and NF transfer pairs (I, tau) */
+template <int NF>
+__device__ __forceinline__ void
+rk4_dyst_rt64(const thermal::Flow &f, const GridParams &g, double *s, double dt)
+{
+	constexpr int ND = 8 + 2 * NF;
+	double k1[ND], k2[ND], k3[ND], k4[ND], t[ND];
+	double hdt = 0.5 * dt;
+	dyst_rhs_rt64<NF>(f, g, s, k1);
+#pragma unroll
+	for(int i = 0; i < ND; ++i) t[i] = fma(hdt, k1[i], s[i]);
+	dyst_rhs_rt64<NF>(f, g, t, k2);
+#pragma unroll
+	for(int i = 0; i < ND; ++i) t[i] = fma(hdt, k2[i], s[i]);
+	dyst_rhs_rt64<NF>(f, g, t, k3);
+#pragma unroll
+	for(int i = 0; i < ND; ++i) t[i] = fma(dt, k3[i], s[i]);
+	dyst_rhs_rt64<NF>(f, g, t, k4);
+	double h6 = dt / 6.0;
+#pragma unroll
+	for(int i = 0; i < ND; ++i)
 		s[i] = fma(h6, fma(2.0, k2[i] + k3[i], k1[i]) + k4[i], s[i]);
 }
 

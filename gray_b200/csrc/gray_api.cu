@@ -94,7 +94,8 @@ check_desc(const gray_render_desc *d)
 		return GRAY_EINVAL;
 	if(d->n_freq < 0 || d->n_freq > GRAY_MAX_FREQ)
 		return GRAY_EINVAL;
-	if(d->flow != GRAY_FLOW_NONE && d->flow != GRAY_FLOW_TORUS)
+	if(d->flow != GRAY_FLOW_NONE && d->flow != GRAY_FLOW_TORUS &&
+	   d->flow != GRAY_FLOW_THERMAL)
 		return GRAY_EINVAL;
 	if(d->term != GRAY_TERM_EPS && d->term != GRAY_TERM_RPLUS)
 		return GRAY_EINVAL;
@@ -102,8 +103,16 @@ check_desc(const gray_render_desc *d)
 		return GRAY_EINVAL;
 	if(d->spacetime != GRAY_ST_KERR && d->spacetime != GRAY_ST_NUMERICAL)
 		return GRAY_EINVAL;
-	if(d->spacetime == GRAY_ST_NUMERICAL && d->n_freq != 0)
-		return GRAY_EINVAL; /* dyst transfer needs the GRMHD flow: not built */
+	/* the torus is an analytic-spacetime model, the thermal flow reads the
+	 * grid's density: each transfer belongs to one kind of spacetime */
+	if(d->n_freq > 0 && d->spacetime == GRAY_ST_NUMERICAL && d->flow != GRAY_FLOW_THERMAL)
+		return GRAY_EINVAL;
+	if(d->n_freq > 0 && d->spacetime == GRAY_ST_KERR && d->flow == GRAY_FLOW_THERMAL)
+		return GRAY_EINVAL;
+	if(d->flow == GRAY_FLOW_THERMAL &&
+	   !(std::isfinite(d->m_adm) && std::isfinite(d->flow_te) && d->flow_te > 0.0 &&
+	     std::isfinite(d->flow_b)))
+		return GRAY_EINVAL;
 	for(int i = 0; i < d->n_freq; ++i)
 		if(!(d->nu[i] > 0.0))
 			return GRAY_EINVAL;
@@ -144,7 +153,12 @@ make_params(const gray_render_desc *d, RenderParams *p)
 		p->nuinv2[i] = 1.0 / (d->nu[i] * d->nu[i]);
 		p->nupow_f[i]  = (float)p->nupow[i];
 		p->nuinv2_f[i] = (float)p->nuinv2[i];
+		p->nu[i] = d->nu[i];
 	}
+	p->m_adm = d->m_adm;
+	p->flow_te = d->flow_te;
+	p->flow_b = d->flow_b;
+	gray_thermal_consts(&p->th);
 }
 
 int
@@ -204,6 +218,26 @@ gi_grid_ready(gray_ctx *c)
 	return grid_ready(c);
 }
 
+/* rt.cl:95-143 constants that need libm, from volatile inputs so that the
+ * compiler folds none of them (the CPU oracle evaluates the same way) */
+void
+gray_thermal_consts(ThermalConsts *t)
+{
+	volatile double three = 3.0, four = 4.0, twelve = 12.0, pi = 3.14159265358979323846,
+	                e_gaunt = 1.78107241799;
+	const double c = 2.99792458e+10, G = 6.67384800e-08, kB = 1.38064881e-16,
+	             me = 9.10938291e-28, msun = 1.98910000e+33;
+	volatile double ff_in = G * msun / (c * c) * 6.8e-38, mec2_kb = me * c * c / kB;
+	volatile double tmax_tmin = 1e+2 / 1e-1;
+	t->g1 = sqrt(three / pi);
+	t->g2 = sqrt(three) / pi;
+	t->g3 = log(four / e_gaunt);
+	t->g4 = log(four / pow(e_gaunt, 2.5));
+	t->g5 = sqrt(twelve);
+	t->ff_f = sqrt(ff_in / (4 * pi * sqrt(mec2_kb)));
+	t->lk_scale = 60.0 / log(tmax_tmin);
+}
+
 int
 gray_internal_check_desc(const gray_render_desc *d)
 {
@@ -232,6 +266,7 @@ gray_strerror(int s)
 	case GRAY_ENOTFOUND: return "unknown render or request id";
 	case GRAY_ESTATE:    return "call out of order";
 	case GRAY_ESIZE:     return "buffer size mismatch";
+	case GRAY_ESOURCE:   return "a caller callback failed";
 	default:             return "unknown status";
 	}
 }
@@ -303,6 +338,10 @@ free_grid(gray_ctx *c)
 	size_t npts = (size_t)g->desc.nx * g->desc.ny * g->desc.nz;
 	for(int l = 0; l < 2; ++l)
 		dfree(c, g->lvl[l], npts * GRAY_NSTRIDE * sizeof(float));
+	if(g->spare)
+		dfree(c, g->spare, npts * GRAY_NSTRIDE * sizeof(float));
+	if(g->staging)
+		cudaFreeHost(g->staging);
 	const int n[3] = {g->desc.nx, g->desc.ny, g->desc.nz};
 	for(int a = 0; a < 3; ++a) {
 		dfree(c, g->nodes[a], (n[a] + 1) * sizeof(double));
@@ -466,8 +505,8 @@ run_mixed(gray_ctx *c, Render *r, double t_init, double dt_dump, long long n_dum
 	if(r->p.spacetime == GRAY_ST_NUMERICAL) {
 		if(!grid_ready(c))
 			return GRAY_ESTATE;
-		CK(launch_dyst_mixed_table(T, c->grid->gp, r->d_queue, r->d_steps, c->stream,
-		                           c->mixed, r->d_steps + 1));
+		CK(launch_dyst_mixed_table(T, c->grid->gp, r->p.n_freq, r->d_queue, r->d_steps,
+		                           c->stream, c->mixed, r->d_steps + 1));
 	} else {
 		CK(launch_mixed_table(T, r->p.n_freq, r->d_queue, r->d_steps, c->stream, c->mixed));
 	}
@@ -914,6 +953,49 @@ gray_swap_levels(gray_ctx *c)
 	return GRAY_OK;
 }
 
+/* internal helpers for the snapshot series (series.cu) */
+Render *
+gi_find_render(gray_ctx *c, int id)
+{
+	return find(c, id);
+}
+
+int
+gi_icond(gray_ctx *c, Render *r)
+{
+	return icond_impl(c, r);
+}
+
+int
+gi_evolve_interval(gray_ctx *c, Render *r, double t, double target, uint64_t n_sub)
+{
+	return evolve_interval(c, r, t, target, n_sub);
+}
+
+int
+gi_check_grid(const gray_grid_desc *g)
+{
+	return check_grid(g);
+}
+
+int
+gi_ensure_grid(gray_ctx *c, const gray_grid_desc *g)
+{
+	return ensure_grid(c, g);
+}
+
+int
+gi_timed_begin(gray_ctx *c)
+{
+	return timed_begin(c);
+}
+
+int
+gi_timed_end(gray_ctx *c, double *ns)
+{
+	return timed_end(c, ns);
+}
+
 /* ---- batches, plans, graphs ---------------------------------------- */
 
 static Batch *
@@ -1036,7 +1118,8 @@ batch_enqueue(gray_ctx *c, Batch *b, const MixedLaunch &cfg, const MixedTable &T
 	}
 	CK(cudaMemsetAsync(b->d_steps, 0, sizeof(unsigned long long), c->stream));
 	if(b->spacetime == GRAY_ST_NUMERICAL)
-		CK(launch_dyst_mixed_table(T, c->grid->gp, b->d_queue, b->d_steps, c->stream, cfg));
+		CK(launch_dyst_mixed_table(T, c->grid->gp, b->n_freq, b->d_queue, b->d_steps,
+		                           c->stream, cfg));
 	else
 		CK(launch_mixed_table(T, b->n_freq, b->d_queue, b->d_steps, c->stream, cfg));
 	return GRAY_OK;

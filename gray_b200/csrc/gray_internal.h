@@ -18,6 +18,19 @@
  * sin/cos (KS.cl:195-197) and of r_+, r_isco and nu^-0.7 keeps all device
  * arithmetic to +, *, fma, /, sqrt, which round identically in the CPU
  * oracle. */
+/* libm-derived constants of the thermal emissivities (rt.cl:95-143),
+ * evaluated once on the host from volatile inputs exactly as the oracle
+ * does, so that no compile-time folding differs between the two. */
+struct ThermalConsts {
+	double g1;        /* sqrt(3/pi)                               */
+	double g2;        /* sqrt(3)/pi                               */
+	double g3;        /* log(4/1.78107241799)                     */
+	double g4;        /* log(4/1.78107241799^2.5)                 */
+	double g5;        /* sqrt(12)                                 */
+	double ff_f;      /* bremsstrahlung normalisation (rt.cl:135) */
+	double lk_scale;  /* T_GRID / log(T_MAX/T_MIN)                */
+};
+
 struct RenderParams {
 	double a, aa;            /* spin and its square                      */
 	double rp, risco;        /* horizon and prograde ISCO radii          */
@@ -31,7 +44,13 @@ struct RenderParams {
 	double nuinv2[GRAY_MAX_FREQ];  /* nu_i^-2   */
 	float  nupow_f[GRAY_MAX_FREQ];
 	float  nuinv2_f[GRAY_MAX_FREQ];
+	/* thermal flow */
+	double nu[GRAY_MAX_FREQ];      /* frequencies (Hz for the thermal flow) */
+	double m_adm, flow_te, flow_b;
+	ThermalConsts th;
 };
+
+void gray_thermal_consts(ThermalConsts *t);
 
 /* Numerical spacetime on the device: two time levels, each interleaved
  * [z][y][x][GRAY_NSTRIDE] floats, plus per-axis fisheye node tables. */
@@ -79,6 +98,7 @@ cudaError_t launch_dyst_icond(const RenderParams &p, const GridParams &g, double
 cudaError_t launch_dyst_evolve64(const RenderParams &p, const GridParams &g, double *data,
                                  double *info, double dt, long long n_sub,
                                  unsigned long long *steps, cudaStream_t st);
+size_t      mixed_render_bytes(void); /* sizeof(MixedRender) */
 cudaError_t launch_boosted_ks(const GridParams &g, float *lvl, double a, double v,
                               int axis, double t, cudaStream_t st);
 

@@ -98,14 +98,23 @@ inside32(const GridParams &g, const float *q)
 }
 
 /* Gamma^mu_ab u^a u^b for mu = t,x,y,z from the 40 interpolated Gamma:
- * corner rows are gathered as float4 and accumulated in f32x2 pairs. */
+ * corner rows are gathered as float4 and accumulated in f32x2 pairs.
+ * With RT, also the covariant momentum k_mu = g_mu,nu u^nu (dyst.cl:55-81,
+ * with the g_zz flag of dyst.cl:78) and n_e = rho (flow.cl:48) into
+ * kn[0..3] and kn[4], contracted per corner like Gamma. */
+template <bool RT = false>
 __device__ __forceinline__ void
-dyst_rhs32(const GridParams &g, const DystConst &dc, const float *s, float *ds)
+dyst_rhs32(const GridParams &g, const DystConst &dc, const float *s, float *ds,
+           float *kn = nullptr)
 {
 	const float *u = s + 4;
 	ds[0] = u[0]; ds[1] = u[1]; ds[2] = u[2]; ds[3] = u[3];
 	if(g.physics && !inside32(g, s)) {
 		ds[4] = ds[5] = ds[6] = ds[7] = 0.0f;
+		if(RT) {
+			kn[0] = -u[0]; kn[1] = u[1]; kn[2] = u[2]; kn[3] = u[3];
+			kn[4] = 0.0f;
+		}
 		return;
 	}
 	int i0[3], i1[3];
@@ -141,6 +150,7 @@ dyst_rhs32(const GridParams &g, const DystConst &dc, const float *s, float *ds)
 	 * corner's 40 Gamma are contracted first (4 sums) and only the sums are
 	 * weighted: 4 accumulators instead of 40 keeps registers for warps. */
 	float Gm[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+	float Km[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
 	const float ax = 1.0f - w[0], ay = 1.0f - w[1], az = 1.0f - w[2];
 	/* a time level whose weight is zero (t outside [t1, t2] in physics
 	 * mode, where the factor is clamped) is not fetched at all */
@@ -172,25 +182,53 @@ dyst_rhs32(const GridParams &g, const DystConst &dc, const float *s, float *ds)
 #pragma unroll
 			for(int m = 0; m < 4; ++m)
 				Gm[m] = fmaf(wl, s[m], Gm[m]);
+			if(RT) {
+				/* g_tt g_tx g_ty g_tz | g_xx g_xy g_xz g_yy | g_yz g_zz rho pad */
+				const float4 a = __ldg(src + 10), b = __ldg(src + 11), d = __ldg(src + 12);
+				const float gzz = g.bug_gzz ? d.x : d.y;
+				const float k0 = fmaf(a.w, u[3], fmaf(a.z, u[2], fmaf(a.y, u[1], a.x * u[0])));
+				const float k1 = fmaf(b.z, u[3], fmaf(b.y, u[2], fmaf(b.x, u[1], a.y * u[0])));
+				const float k2 = fmaf(d.x, u[3], fmaf(b.w, u[2], fmaf(b.y, u[1], a.z * u[0])));
+				const float k3 = fmaf(gzz, u[3], fmaf(d.x, u[2], fmaf(b.z, u[1], a.w * u[0])));
+				Km[0] = fmaf(wl, k0, Km[0]);
+				Km[1] = fmaf(wl, k1, Km[1]);
+				Km[2] = fmaf(wl, k2, Km[2]);
+				Km[3] = fmaf(wl, k3, Km[3]);
+				Km[4] = fmaf(wl, d.z, Km[4]);
+			}
 		}
 	}
 #pragma unroll
 	for(int m = 0; m < 4; ++m)
 		ds[4 + m] = fmaf(Gm[0], u[m], -Gm[m]);
+	if(RT) {
+#pragma unroll
+		for(int m = 0; m < 5; ++m)
+			kn[m] = Km[m];
+	}
 }
 
-__global__ void __launch_bounds__(256, 2)
+/* NF > 0: the thermal transfer pairs (I, tau) ride along in FP64 (rt[],
+ * first the NF intensities, then the NF optical depths), integrated by the
+ * same RK4 stages with the FP64 emissivities of thermal.cuh on the FP32
+ * momentum and density; the stages run as a rolled loop so that the FP64
+ * transfer is instantiated once. */
+template <int NF>
+__global__ void __launch_bounds__(256, NF == 0 ? 2 : 1)
 dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
                   unsigned int *__restrict__ queue, unsigned long long *__restrict__ steps,
                   unsigned long long *__restrict__ inbox)
 {
-	constexpr int ND = 8;
+	constexpr int ND = 8;            /* FP32 geodesic state           */
+	constexpr int NR = 2 * NF;       /* FP64 transfer state           */
 	const unsigned FULL = 0xffffffffu;
 	const int lane = threadIdx.x & 31;
 	float hi[ND], lo[ND];
+	double rt[NR > 0 ? NR : 1];
 	long long ray = 0;
 	int dump = 0, h = 0, dh_step = 0, n = 0;
 	float dtn = 0.0f;
+	double dtnd = 0.0; /* the FP64 substep unit of the transfer */
 	bool active = false, exhausted = false;
 	unsigned long long cnt = 0, cnt_in = 0; /* all steps; steps that interpolate */
 	const MixedRender *c = nullptr;
@@ -220,6 +258,9 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 						hi[k] = (float)v;
 						lo[k] = (float)((double)hi[k] - v);
 					}
+#pragma unroll
+					for(int k = 0; k < NR; ++k)
+						rt[k] = c->data[(ND + k) * c->n_rays + ray];
 					dump = c->dump_begin - 1;
 					h = n; /* forces the first dump set-up below */
 					active = true;
@@ -240,6 +281,9 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 					s[k] = (double)hi[k] - (double)lo[k];
 					c->data[k * c->n_rays + ray] = s[k];
 				}
+#pragma unroll
+				for(int k = 0; k < NR; ++k)
+					c->data[(ND + k) * c->n_rays + ray] = rt[k];
 				c->info[ray] = dyst_getuu64(g, s);
 				active = false;
 				continue;
@@ -248,7 +292,8 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 			double t1 = c->t_init + (double)(dump + 1) * c->dt_dump;
 			double dt = t1 - t0;
 			dh_step = (int)(dyst_getdt64(dt / (double)c->n_sub) / dt * (double)n);
-			dtn = (float)(dt / (double)n);
+			dtnd = dt / (double)n;
+			dtn = (float)dtnd;
 			h = 0;
 			if(dh_step <= 0) { /* zero-length interval: nothing to integrate */
 				h = n;
@@ -259,6 +304,41 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 		const float hs = (float)dh * dtn, hh = 0.5f * hs;
 		float k[ND], t[ND], sum[ND];
 		cnt_in += (!g.physics || inside32(g, hi)) ? 1 : 0;
+		if constexpr(NF > 0) {
+			const thermal::Flow fl = {c->nu_hz, c->m_adm, c->flow_te, c->flow_b, &c->th};
+			const double hsd = (double)dh * dtnd;
+			double trt[NR], srt[NR], krt[NR];
+#pragma unroll
+			for(int i = 0; i < ND; ++i)
+				t[i] = hi[i];
+#pragma unroll
+			for(int i = 0; i < NR; ++i)
+				trt[i] = rt[i];
+#pragma unroll 1
+			for(int st = 0; st < 4; ++st) {
+				float kn[5];
+				dyst_rhs32<true>(g, dc, t, k, kn);
+				const double kd[4] = {kn[0], kn[1], kn[2], kn[3]};
+				thermal::rt_rhs<NF>(fl, kd, (double)kn[4], trt + NF, krt, krt + NF);
+				const float wg = (st == 1 || st == 2) ? 2.0f : 1.0f;
+				const float cg = st < 2 ? hh : hs;
+				const double wd = wg, cd = st < 2 ? 0.5 * hsd : hsd;
+#pragma unroll
+				for(int i = 0; i < ND; ++i) { /* k4 stays in k for the update */
+					if(st < 3)
+						sum[i] = st == 0 ? k[i] : fmaf(wg, k[i], sum[i]);
+					t[i] = fmaf(cg, k[i], hi[i]);
+				}
+#pragma unroll
+				for(int i = 0; i < NR; ++i) {
+					srt[i] = st == 0 ? krt[i] : fma(wd, krt[i], srt[i]);
+					trt[i] = fma(cd, krt[i], rt[i]);
+				}
+			}
+#pragma unroll
+			for(int i = 0; i < NR; ++i)
+				rt[i] = fma(hsd / 6.0, srt[i], rt[i]);
+		} else {
 		dyst_rhs32(g, dc, hi, k);
 #pragma unroll
 		for(int i = 0; i < ND; ++i) {
@@ -278,6 +358,7 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 			t[i] = fmaf(hs, k[i], hi[i]);
 		}
 		dyst_rhs32(g, dc, t, k);
+		}
 		const float h6 = hs * (1.0f / 6.0f);
 		bool bad = false;
 #pragma unroll
@@ -298,6 +379,9 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 				s[kk] = (double)hi[kk] - (double)lo[kk];
 				c->data[kk * c->n_rays + ray] = s[kk];
 			}
+#pragma unroll
+			for(int kk = 0; kk < NR; ++kk)
+				c->data[(ND + kk) * c->n_rays + ray] = rt[kk];
 			c->info[ray] = s[0] - s[0]; /* NaN marks the ray */
 			active = false;
 		}
@@ -313,31 +397,19 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 		atomicAdd(inbox, cnt_in);
 }
 
-[[maybe_unused]] inline unsigned
-blocks_for(long long n, int block)
-{
-	return (unsigned)((n + block - 1) / block);
-}
-
-} /* namespace */
-
+template <int NF>
 cudaError_t
-launch_dyst_mixed_table(const MixedTable &T, const GridParams &g, unsigned int *queue,
-                        unsigned long long *steps, cudaStream_t st, const MixedLaunch &cfg,
-                        unsigned long long *inbox)
+launch_dyst_nf(const MixedTable &T, const GridParams &g, const DystConst &dc,
+               unsigned int *queue, unsigned long long *steps, cudaStream_t st,
+               const MixedLaunch &cfg, unsigned long long *inbox)
 {
-	DystConst dc;
-	for(int a = 0; a < 3; ++a) {
-		dc.B[a] = (float)g.B[a];
-		dc.iA[a] = (float)(1.0 / g.A[a]);
-	}
-	cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned int), st);
-	if(e != cudaSuccess)
-		return e;
 	int block = cfg.block > 0 ? cfg.block : 256;
+	if(block > 256)
+		return cudaErrorInvalidValue; /* __launch_bounds__(256) */
 	int per_sm = cfg.blocks_per_sm;
 	if(per_sm <= 0) {
-		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dyst_mixed_kernel, block, 0);
+		cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+			&per_sm, dyst_mixed_kernel<NF>, block, 0);
 		if(e != cudaSuccess)
 			return e;
 		if(per_sm <= 0)
@@ -348,7 +420,38 @@ launch_dyst_mixed_table(const MixedTable &T, const GridParams &g, unsigned int *
 	unsigned grid = (unsigned)(want < need ? want : need);
 	if(grid == 0)
 		grid = 1;
-	dyst_mixed_kernel<<<grid, block, 0, st>>>(T, g, dc, queue, steps, inbox);
+	dyst_mixed_kernel<NF><<<grid, block, 0, st>>>(T, g, dc, queue, steps, inbox);
 	return cudaGetLastError();
+}
+
+} /* namespace */
+
+cudaError_t
+launch_dyst_mixed_table(const MixedTable &T, const GridParams &g, int n_freq,
+                        unsigned int *queue, unsigned long long *steps, cudaStream_t st,
+                        const MixedLaunch &cfg, unsigned long long *inbox)
+{
+	static_assert(GRAY_MAX_FREQ == 8, "one instantiation per frequency count");
+	DystConst dc;
+	for(int a = 0; a < 3; ++a) {
+		dc.B[a] = (float)g.B[a];
+		dc.iA[a] = (float)(1.0 / g.A[a]);
+	}
+	if(n_freq < 0 || n_freq > GRAY_MAX_FREQ)
+		return cudaErrorInvalidValue;
+	cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned int), st);
+	if(e != cudaSuccess)
+		return e;
+	switch(n_freq) {
+	case 0: return launch_dyst_nf<0>(T, g, dc, queue, steps, st, cfg, inbox);
+	case 1: return launch_dyst_nf<1>(T, g, dc, queue, steps, st, cfg, inbox);
+	case 2: return launch_dyst_nf<2>(T, g, dc, queue, steps, st, cfg, inbox);
+	case 3: return launch_dyst_nf<3>(T, g, dc, queue, steps, st, cfg, inbox);
+	case 4: return launch_dyst_nf<4>(T, g, dc, queue, steps, st, cfg, inbox);
+	case 5: return launch_dyst_nf<5>(T, g, dc, queue, steps, st, cfg, inbox);
+	case 6: return launch_dyst_nf<6>(T, g, dc, queue, steps, st, cfg, inbox);
+	case 7: return launch_dyst_nf<7>(T, g, dc, queue, steps, st, cfg, inbox);
+	default: return launch_dyst_nf<8>(T, g, dc, queue, steps, st, cfg, inbox);
+	}
 }
 

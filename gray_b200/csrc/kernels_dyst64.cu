@@ -39,22 +39,27 @@ dyst_icond_kernel(const RenderParams p, const GridParams g, double *__restrict__
 #pragma unroll
 	for(int c = 0; c < 8; ++c)
 		data[c * n + r] = s[c];
+	for(int c = 8; c < p.n_data; ++c)
+		data[c * n + r] = 0.0; /* rt_icond(), rt.cl:179-183 */
 	info[r] = dyst_getuu64(g, s);
 }
 
-/* driver.cl:69-108 on the numerical spacetime */
+/* driver.cl:69-108 on the numerical spacetime, with NF transfer pairs */
+template <int NF>
 __global__ void __launch_bounds__(128)
-dyst_evolve64_kernel(const RenderParams p, const GridParams g, double *__restrict__ data,
-                     double *__restrict__ info, const double dt, const long long n_sub,
-                     unsigned long long *__restrict__ steps)
+dyst_evolve64_kernel(const __grid_constant__ RenderParams p, const GridParams g,
+                     double *__restrict__ data, double *__restrict__ info, const double dt,
+                     const long long n_sub, unsigned long long *__restrict__ steps)
 {
+	constexpr int ND = 8 + 2 * NF;
 	const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
 	const long long nr = p.n_rays;
+	const thermal::Flow f = {p.nu, p.m_adm, p.flow_te, p.flow_b, &p.th};
 	unsigned long long cnt = 0;
 	if(r < nr) {
-		double s[8];
+		double s[ND];
 #pragma unroll
-		for(int c = 0; c < 8; ++c)
+		for(int c = 0; c < ND; ++c)
 			s[c] = data[c * nr + r];
 		const int n = (int)((INT_MAX / n_sub) * n_sub);
 		const double dts = dt / (double)n_sub;
@@ -65,11 +70,14 @@ dyst_evolve64_kernel(const RenderParams p, const GridParams g, double *__restric
 				break;
 			if(dh > n - h)
 				dh = n - h;
-			rk4_dyst64(g, s, ((double)dh * dt) / (double)n);
+			if(NF == 0)
+				rk4_dyst64(g, s, ((double)dh * dt) / (double)n);
+			else
+				rk4_dyst_rt64<NF>(f, g, s, ((double)dh * dt) / (double)n);
 			++cnt;
 		}
 #pragma unroll
-		for(int c = 0; c < 8; ++c)
+		for(int c = 0; c < ND; ++c)
 			data[c * nr + r] = s[c];
 		info[r] = dyst_getuu64(g, s);
 	}
@@ -201,8 +209,19 @@ cudaError_t
 launch_dyst_evolve64(const RenderParams &p, const GridParams &g, double *data, double *info,
                      double dt, long long n_sub, unsigned long long *steps, cudaStream_t st)
 {
-	dyst_evolve64_kernel<<<blocks_for(p.n_rays, 128), 128, 0, st>>>(p, g, data, info, dt,
-	                                                                n_sub, steps);
+	const unsigned nb = blocks_for(p.n_rays, 128);
+	switch(p.n_freq) {
+#define GRAY_DYST64_CASE(NF)                                                             \
+	case NF:                                                                         \
+		dyst_evolve64_kernel<NF><<<nb, 128, 0, st>>>(p, g, data, info, dt, n_sub, steps); \
+		break;
+	GRAY_DYST64_CASE(0) GRAY_DYST64_CASE(1) GRAY_DYST64_CASE(2) GRAY_DYST64_CASE(3)
+	GRAY_DYST64_CASE(4) GRAY_DYST64_CASE(5) GRAY_DYST64_CASE(6) GRAY_DYST64_CASE(7)
+	GRAY_DYST64_CASE(8)
+#undef GRAY_DYST64_CASE
+	default:
+		return cudaErrorInvalidValue;
+	}
 	return cudaGetLastError();
 }
 

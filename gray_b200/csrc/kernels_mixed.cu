@@ -727,4 +727,17 @@ fill_mixed_render(const RenderParams &p, double *data, double *info, double t_in
 	m->t_init = t_init;
 	m->dt_dump = dt_dump;
 	m->n_sub = n_sub;
+	for(int i = 0; i < GRAY_MAX_FREQ; ++i)
+		m->nu_hz[i] = p.nu[i];
+	m->m_adm = p.m_adm;
+	m->flow_te = p.flow_te;
+	m->flow_b = p.flow_b;
+	m->th = p.th;
+	m->thermal = p.flow == GRAY_FLOW_THERMAL;
+}
+
+size_t
+mixed_render_bytes(void)
+{
+	return sizeof(MixedRender);
 }

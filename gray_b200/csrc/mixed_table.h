@@ -23,6 +23,11 @@ struct MixedRender {
 	long long n_rays;
 	double t_init, dt_dump;    /* dump i covers [t_init + i dt, t_init + (i+1) dt] */
 	long long n_sub;
+	/* thermal flow of numerical renders (FP64 transfer) */
+	double nu_hz[GRAY_MAX_FREQ];
+	double m_adm, flow_te, flow_b;
+	ThermalConsts th;
+	int    thermal;
 };
 
 struct MixedTable {
@@ -41,9 +46,10 @@ cudaError_t launch_mixed_table(const MixedTable &T, int n_freq, unsigned int *qu
                                unsigned long long *steps, cudaStream_t st,
                                const MixedLaunch &cfg);
 
-/* numerical spacetime: every render of the table on the same grid; inbox
- * (nullable) accumulates the steps that interpolate the grid */
-cudaError_t launch_dyst_mixed_table(const MixedTable &T, const GridParams &g,
+/* numerical spacetime: every render of the table on the same grid and with
+ * the same n_freq; inbox (nullable) accumulates the steps that interpolate
+ * the grid */
+cudaError_t launch_dyst_mixed_table(const MixedTable &T, const GridParams &g, int n_freq,
                                     unsigned int *queue, unsigned long long *steps,
                                     cudaStream_t st, const MixedLaunch &cfg,
                                     unsigned long long *inbox = nullptr);

@@ -32,8 +32,10 @@
 
 namespace {
 
-constexpr int GROUPS = GRAY_MAX_FREQ + 2; /* analytic n_freq 0..8, numerical */
+/* one table per kind and frequency count: analytic n_freq 0..8 are groups
+ * 0..8, numerical n_freq 0..8 are groups 9..17 */
 constexpr int NUM_GROUP = GRAY_MAX_FREQ + 1;
+constexpr int GROUPS = 2 * NUM_GROUP;
 
 double
 now_s()
@@ -56,7 +58,10 @@ struct Request {
 	std::atomic<bool> cancel{false}; /* set by gray_serve_cancel, read by the scheduler */
 	std::vector<double> h_data, h_info;
 
-	int group() const { return p.spacetime == GRAY_ST_NUMERICAL ? NUM_GROUP : p.n_freq; }
+	int group() const
+	{
+		return p.spacetime == GRAY_ST_NUMERICAL ? NUM_GROUP + p.n_freq : p.n_freq;
+	}
 };
 
 } /* namespace */
@@ -122,8 +127,8 @@ iterate(Server *S, std::vector<Request *> &fresh)
 			continue;
 		}
 		r->d_info = r->d_data + (size_t)r->p.n_rays * r->p.n_data;
-		cudaStream_t st_ = S->s[r->group() == NUM_GROUP ? 1 : 0];
-		e = r->group() == NUM_GROUP
+		cudaStream_t st_ = S->s[r->group() >= NUM_GROUP ? 1 : 0];
+		e = r->group() >= NUM_GROUP
 		        ? launch_dyst_icond(r->p, c->grid->gp, r->d_data, r->d_info, st_)
 		        : launch_icond64(r->p, r->d_data, r->d_info, st_);
 		if(e != cudaSuccess)
@@ -179,10 +184,11 @@ iterate(Server *S, std::vector<Request *> &fresh)
 		T.n_renders = count[g];
 		T.total = total[g];
 		unsigned int *q = (unsigned int *)((char *)S->d_queue + 64 * g);
-		if(g == NUM_GROUP) {
+		if(g >= NUM_GROUP) {
 			MixedLaunch dc = cfg;
 			dc.block = 256;
-			e = launch_dyst_mixed_table(T, c->grid->gp, q, S->d_steps + g, S->s[1], dc);
+			e = launch_dyst_mixed_table(T, c->grid->gp, g - NUM_GROUP, q, S->d_steps + g,
+			                            S->s[1], dc);
 		} else {
 			e = launch_mixed_table(T, g, q, S->d_steps + g, S->s[0], cfg);
 		}
@@ -237,7 +243,7 @@ iterate(Server *S, std::vector<Request *> &fresh)
 		S->stats.iterations++;
 		S->stats.busy_s += ms * 1e-3;
 		for(int g = 0; g < GROUPS; ++g)
-			S->stats.ray_steps[g == NUM_GROUP ? 1 : 0] += S->h_steps[g];
+			S->stats.ray_steps[g >= NUM_GROUP ? 1 : 0] += S->h_steps[g];
 	}
 	S->cv.notify_all();
 	return GRAY_OK;

@@ -14,7 +14,8 @@
  *   sim-org/param.opts:4-18 M_ADM:m dyst_file:data enable_fast_light:fast_light
  *                           n_electron:ne beta_crit:bc R_high:Rh R_low:Rl nu
  * plus the options of the analytic torus (flow, torus_n0, torus_kappa,
- * torus_hr) and the stop rule (term).  conf() follows the lux convention:
+ * torus_hr), of the thermal flow (flow_te:te, flow_b:b; flow.cl:51-52 fixes
+ * them at 1e12 and 0) and the stop rule (term).  conf() follows the lux convention:
  * 0 when the argument was consumed (sim/gray.c:37-73).
  *
  * init() replaces sim/gray.c:75-151 (device, ray buffer, initcond, planner);
@@ -67,6 +68,7 @@ struct gray_job {
 	/* analytic torus and stop rule */
 	char     flow[16];
 	double   torus_n0, torus_kappa, torus_hr;
+	double   flow_te, flow_b;
 	char     term[16];
 
 	/* run time */
@@ -126,6 +128,8 @@ static const opt OPTS[] = {
 	{"torus_n0",             T_DBL,  OFF(torus_n0), SZ(torus_n0), "1"},
 	{"torus_kappa",          T_DBL,  OFF(torus_kappa), SZ(torus_kappa), "1"},
 	{"torus_hr",             T_DBL,  OFF(torus_hr), SZ(torus_hr), "0.3"},
+	{"flow_te:te",           T_DBL,  OFF(flow_te), SZ(flow_te), "1e12"},
+	{"flow_b:b",             T_DBL,  OFF(flow_b), SZ(flow_b), "0"},
 	{"term",                 T_STR,  OFF(term), SZ(term), "eps"},
 };
 #define N_OPTS (sizeof(OPTS) / sizeof(OPTS[0]))
@@ -311,7 +315,13 @@ gray_job_desc(const gray_lux_job *ego, gray_render_desc *d)
 	d->n_freq = j->n_freq;
 	for(int i = 0; i < j->n_freq; ++i)
 		d->nu[i] = j->nu[i];
-	d->flow = (j->n_freq && !strcmp(j->flow, "torus")) ? GRAY_FLOW_TORUS : GRAY_FLOW_NONE;
+	d->flow = !j->n_freq                   ? GRAY_FLOW_NONE
+	          : !strcmp(j->flow, "torus")   ? GRAY_FLOW_TORUS
+	          : !strcmp(j->flow, "thermal") ? GRAY_FLOW_THERMAL
+	                                        : GRAY_FLOW_NONE;
+	d->m_adm = j->M_ADM;
+	d->flow_te = j->flow_te;
+	d->flow_b = j->flow_b;
 	d->torus_n0 = j->torus_n0;
 	d->torus_kappa = j->torus_kappa;
 	d->torus_hr = j->torus_hr;

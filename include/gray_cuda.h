@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define GRAY_ABI_VERSION 1
+#define GRAY_ABI_VERSION 2
 #define GRAY_MAX_FREQ    8
 
 enum gray_status {
@@ -39,7 +39,8 @@ enum gray_status {
 	GRAY_ETIMEOUT  = -6,  /* bounded device wait ran out           */
 	GRAY_ENOTFOUND = -7,  /* unknown render / request id           */
 	GRAY_ESTATE    = -8,  /* call out of order (e.g. no icond yet) */
-	GRAY_ESIZE     = -9   /* host buffer size does not match       */
+	GRAY_ESIZE     = -9,  /* host buffer size does not match       */
+	GRAY_ESOURCE   = -10  /* a caller callback reported failure    */
 };
 
 enum gray_precision {
@@ -53,8 +54,13 @@ enum gray_spacetime {
 };
 
 enum gray_flow {
-	GRAY_FLOW_NONE  = 0,   /* geodesics only (n_freq ignored)               */
-	GRAY_FLOW_TORUS = 1    /* analytic power-law torus feeding rt.cl form   */
+	GRAY_FLOW_NONE    = 0, /* geodesics only (n_freq ignored)               */
+	GRAY_FLOW_TORUS   = 1, /* analytic power-law torus feeding rt.cl form   */
+	GRAY_FLOW_THERMAL = 2  /* the reference's template flow (flow.cl:36-58):
+	                          n_e = rho of the grid, T_e = flow_te, |b| =
+	                          flow_b along z, fluid at rest; thermal
+	                          bremsstrahlung + synchrotron of rt.cl:28-198
+	                          (numerical spacetimes)                       */
 };
 
 enum gray_term {
@@ -96,6 +102,10 @@ typedef struct gray_render_desc {
 	/* selection */
 	int32_t  spacetime;       /* enum gray_spacetime                          */
 	int32_t  precision;       /* enum gray_precision                          */
+	/* thermal flow (GRAY_FLOW_THERMAL) */
+	double   m_adm;           /* param.opts M_ADM:m, solar masses            */
+	double   flow_te;         /* electron temperature kT/(m_e c^2) (1e12)     */
+	double   flow_b;          /* magnetic field magnitude, along z (0)        */
 } gray_render_desc;
 
 typedef struct gray_ctx gray_ctx;
@@ -315,7 +325,7 @@ int gray_read_spacetime(gray_ctx *ctx, int level, float *fields, size_t bytes);
  *    stream).  If steps_host is non-NULL the call waits and stores the
  *    accepted ray-steps there; otherwise it returns after enqueueing. */
 #define GRAY_NOALLOC_MAX_RENDERS   32
-#define GRAY_NOALLOC_SCRATCH_BYTES 8192
+#define GRAY_NOALLOC_SCRATCH_BYTES 16384
 int gray_run_mixed_noalloc(int device, const gray_render_desc *descs, int n_renders,
                            double *const *state_dev, double *const *info_dev,
                            void *cuda_stream, uint64_t *steps_host);

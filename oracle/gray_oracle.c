@@ -706,6 +706,157 @@ pairs10(const double u[4], double p[10])
 		}
 }
 
+/* ------------------------------------------------------------------------ */
+/* Thermal emissivities (rt.cl:28-170) and the template flow (flow.cl)       */
+/* ------------------------------------------------------------------------ */
+
+/* CGS constants of rt.cl:28-36 */
+#define C_c    2.99792458e+10
+#define C_h    6.62606957e-27
+#define C_G    6.67384800e-08
+#define C_kB   1.38064881e-16
+#define C_Ry   2.17987197e-11
+#define C_e    4.80320425e-10
+#define C_me   9.10938291e-28
+#define C_mSun 1.98910000e+33
+#define O_PI   3.14159265358979323846
+#define O_SQRT2 1.41421356237309504880
+#define T_MIN  1e-1
+#define T_MAX  1e+2
+#define T_GRID 60
+
+#include "../gray_b200/csrc/logk2_table.h"
+static const double LOGK2[GRAY_LOGK2_N] = {GRAY_LOGK2_VALUES};
+
+/* Constants that need libm, evaluated at run time from volatile inputs
+ * (no compile-time folding), exactly as the library's host code does. */
+typedef struct {
+	double g1, g2, g3, g4, g5, ff_f, lk_scale;
+} th_consts;
+
+static void
+th_setup(th_consts *t)
+{
+	volatile double three = 3.0, four = 4.0, twelve = 12.0, pi = O_PI, e_gaunt = 1.78107241799;
+	volatile double ff_in = C_G * C_mSun / (C_c * C_c) * 6.8e-38, mec2_kb = C_me * C_c * C_c / C_kB;
+	volatile double tmax_tmin = T_MAX / T_MIN;
+	t->g1 = sqrt(three / pi);
+	t->g2 = sqrt(three) / pi;
+	t->g3 = log(four / e_gaunt);
+	t->g4 = log(four / pow(e_gaunt, 2.5));
+	t->g5 = sqrt(twelve);
+	t->ff_f = sqrt(ff_in / (4 * pi * sqrt(mec2_kb)));
+	t->lk_scale = (double)T_GRID / log(tmax_tmin);
+}
+
+static th_consts TH;
+
+/* set up once when the library loads, before any OpenMP region reads it */
+__attribute__((constructor)) static void
+th_init(void)
+{
+	th_setup(&TH);
+}
+
+static const th_consts *
+th(void)
+{
+	return &TH;
+}
+
+/* rt.cl:70-78; the index is kept inside the table (te == T_MAX exactly
+ * would read one entry past its end in the reference) */
+double
+orc_log_K2it(double te)
+{
+	const double h = log(te / T_MIN) * th()->lk_scale;
+	int i = (int)h;
+	if(i > T_GRID - 1)
+		i = T_GRID - 1;
+	const double d = h - i;
+	return (1 - d) * LOGK2[i] + d * LOGK2[i + 1];
+}
+
+/* rt.cl:80-93 */
+double
+orc_B_Planck(double nu, double te)
+{
+	double f1 = 2 * C_h * C_c;
+	double f2 = C_h / (C_me * C_c);
+	nu /= C_c;
+	f1 *= nu * nu;
+	f2 *= nu / (te + ORC_EPSILON);
+	return nu * (f2 > 1e-5 ? f1 / (exp(f2) - 1) : (f1 / f2) / (1 + f2 / 2 + f2 * f2 / 6));
+}
+
+/* rt.cl:95-120 */
+double
+orc_Gaunt(double x, double y)
+{
+	const th_consts *t = th();
+	const double sx = sqrt(x);
+	const double sy = sqrt(y);
+	if(x > 1)
+		return y > 1 ? t->g1 / sy : t->g2 * (t->g3 - log(y + ORC_EPSILON));
+	else if(x * y > 1)
+		return t->g5 / (sx * sy);
+	else if(y > sx)
+		return 1;
+	else {
+		const double g = t->g2 * (t->g4 + log(sx / (y + ORC_EPSILON)));
+		return g > ORC_EPSILON ? g : ORC_EPSILON;
+	}
+}
+
+/* rt.cl:122-143 (M_ADM passed in) */
+double
+orc_L_j_ff(double m_adm, double nu, double te, double ne)
+{
+	double x = C_me * C_c * C_c / C_Ry;
+	double y = C_h / (C_me * C_c * C_c);
+	double f = th()->ff_f;
+	x *= te;
+	y *= nu / te;
+	f *= ne;
+	return (m_adm * f * orc_Gaunt(x, y)) * (f / (sqrt(te) * exp(y) + ORC_EPSILON));
+}
+
+/* rt.cl:145-170 */
+double
+orc_L_j_syn(double m_adm, double nu, double te, double ne, double b, double cos_theta)
+{
+	if(te <= T_MIN || cos_theta <= -1 || cos_theta >= 1)
+		return 0;
+	const double nus = te * te * b * sqrt(1 - cos_theta * cos_theta) *
+	                   (C_e / (9 * O_PI * C_me * C_c));
+	const double x = nu / (nus + ORC_EPSILON);
+	const double f = (C_G * C_mSun / (C_c * C_c)) * (O_SQRT2 * O_PI * C_e * C_e / (3 * C_c));
+	const double cbrtx = cbrt(x);
+	const double xx = sqrt(x) + 1.88774862536 * sqrt(cbrtx);
+	const double log_K2 = (te > T_MAX) ? log(2 * te * te - 0.5) : orc_log_K2it(te);
+	return (m_adm * xx * exp(-cbrtx)) * (xx * exp(-log_K2)) * (f * ne * nus);
+}
+
+/* rt.cl:185-198 with the template flow of flow.cl:36-58 generalised to a
+ * field of magnitude b along z: shift = -k.u with u = (1,0,0,0),
+ * cos = k.b / (shift |b|). */
+static void
+thermal_rt(const orc_desc *d, const double k[4], double ne, const double *s, double *ds)
+{
+	const int nf = d->n_freq;
+	const double te = d->flow_te, b = d->flow_b;
+	const double shift = -k[0];
+	const double bkcos = (k[3] * b) / (shift * b + ORC_EPSILON);
+	for(int i = 0; i < nf; ++i) {
+		const double nu = d->nu[i] * shift;
+		const double B_nu = orc_B_Planck(nu, te);
+		const double L = orc_L_j_syn(d->m_adm, nu, te, ne, b, bkcos) +
+		                 orc_L_j_ff(d->m_adm, nu, te, ne);
+		ds[8 + i]      = -L * exp(-s[8 + nf + i]) / (shift * shift + ORC_EPSILON);
+		ds[8 + nf + i] = -L * shift / (B_nu + ORC_EPSILON);
+	}
+}
+
 /* dyst.cl:112-194: a^mu = -Gamma^mu_ab u^a u^b + (Gamma^t_ab u^a u^b) u^mu */
 void
 orc_dyst_rhs(const orc_grid *g, const double s[8], double ds[8])
@@ -762,14 +913,58 @@ orc_dyst_getdt(double dt)
 	return dt;
 }
 
+/* phys.cl:66-74 on the numerical spacetime: the geodesic, and for the
+ * thermal flow the transfer with k = down(q, u) (dyst.cl:55-81) and n_e the
+ * interpolated rho (flow.cl:48).  One interpolation serves all fields
+ * (the reference interpolates them field by field: same values).  In
+ * physics mode outside the box the spacetime is flat and n_e = 0. */
+void
+orc_dyst_rhs_rt(const orc_desc *d, const orc_grid *g, const double *s, double *ds)
+{
+	const double *u = s + 4;
+	const int nf = d->n_freq;
+	if(nf == 0 || d->flow != ORC_FLOW_THERMAL) {
+		orc_dyst_rhs(g, s, ds);
+		for(int i = 0; i < 2 * nf; ++i)
+			ds[8 + i] = 0.0;
+		return;
+	}
+	double v[ORC_NCOMP], k[4], ne;
+	ds[0] = u[0]; ds[1] = u[1]; ds[2] = u[2]; ds[3] = u[3];
+	if(g->physics && !inside_box(g, s)) {
+		ds[4] = ds[5] = ds[6] = ds[7] = 0.0;
+		k[0] = -u[0]; k[1] = u[1]; k[2] = u[2]; k[3] = u[3];
+		ne = 0.0;
+	} else {
+		double p[10], G[4], c[10], M[4][4];
+		interp_all(g, s, v);
+		pairs10(u, p);
+		for(int m = 0; m < 4; ++m)
+			G[m] = quad10(v + 10 * m, p);
+		for(int m = 0; m < 4; ++m)
+			ds[4 + m] = fma(G[0], u[m], -G[m]);
+		for(int i = 0; i < 10; ++i)
+			c[i] = v[40 + i];
+		if(g->bug_gzz)
+			c[9] = c[8];
+		sym10(c, M);
+		for(int i = 0; i < 4; ++i)
+			k[i] = dot4(M[i], u);
+		ne = v[50];
+	}
+	thermal_rt(d, k, ne, s, ds);
+}
+
 typedef struct {
+	const orc_desc *d;
 	const orc_grid *g;
 } dyst_ctx;
 
 static void
 dyst_fn(const void *ctx, const double *s, double *ds)
 {
-	orc_dyst_rhs(((const dyst_ctx *)ctx)->g, s, ds);
+	const dyst_ctx *c = (const dyst_ctx *)ctx;
+	orc_dyst_rhs_rt(c->d, c->g, s, ds);
 }
 
 int64_t
@@ -778,17 +973,16 @@ orc_dyst_evolve_ray(const orc_desc *d, const orc_grid *g, double *s, double dt,
 {
 	const int n = (int)((INT_MAX / n_sub) * n_sub);
 	const double dts = dt / (double)n_sub;
-	dyst_ctx c = {g};
+	dyst_ctx c = {d, g};
 	int64_t steps = 0;
 	int h, dh;
-	(void)d;
 	for(h = 0; h < n; h += dh) {
 		dh = (int)(orc_dyst_getdt(dts) / dt * (double)n);
 		if(!dh)
 			break;
 		if(dh > n - h)
 			dh = n - h;
-		rk4(dyst_fn, &c, 8, s, ((double)dh * dt) / (double)n);
+		rk4(dyst_fn, &c, 8 + 2 * d->n_freq, s, ((double)dh * dt) / (double)n);
 		++steps;
 	}
 	return steps;
@@ -799,6 +993,9 @@ orc_dyst_trace(const orc_desc *d, const orc_grid *g, const int64_t *rays,
                int64_t n, double *out, double *info, int64_t *steps, int nthreads)
 {
 	double cam[4];
+	const int nd = 8 + 2 * d->n_freq;
+	if(d->n_freq < 0 || d->n_freq > ORC_MAX_FREQ || d->n_sub <= 0)
+		return -1;
 	orc_camera(d, cam);
 #ifdef _OPENMP
 	if(nthreads <= 0)
@@ -806,9 +1003,11 @@ orc_dyst_trace(const orc_desc *d, const orc_grid *g, const int64_t *rays,
 #pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
 #endif
 	for(int64_t j = 0; j < n; ++j) {
-		double *s = out + j * 8;
+		double *s = out + j * nd;
 		int64_t st = 0;
 		orc_dyst_icond(d, cam, rays[j], s);
+		for(int i = 0; i < 2 * d->n_freq; ++i)
+			s[8 + i] = 0.0; /* rt.cl:179-183 */
 		for(int64_t i = 0; i < d->n_dump; ) {
 			double t      = d->t_init + (double)i * d->dt_dump;
 			double target = d->t_init + (double)(++i) * d->dt_dump;

@@ -34,8 +34,9 @@ extern "C" {
  * r < 1.01 r_+. */
 enum { ORC_TERM_EPS = 0, ORC_TERM_RPLUS = 1 };
 
-/* Flow models feeding the transfer equation. */
-enum { ORC_FLOW_NONE = 0, ORC_FLOW_TORUS = 1 };
+/* Flow models feeding the transfer equation. ORC_FLOW_THERMAL is the
+ * reference's template flow (flow.cl:36-58) with rt.cl's emissivities. */
+enum { ORC_FLOW_NONE = 0, ORC_FLOW_TORUS = 1, ORC_FLOW_THERMAL = 2 };
 
 typedef struct {
 	/* Kerr.opts */
@@ -52,6 +53,8 @@ typedef struct {
 	double  nu[ORC_MAX_FREQ];
 	int     flow;
 	double  torus_n0, torus_kappa, torus_hr;
+	/* thermal flow: M_ADM (param.opts:5), T_e (flow.cl:49), |b| along z */
+	double  m_adm, flow_te, flow_b;
 } orc_desc;
 
 /* Numerical spacetime grid (interp.cl / dyst.cl).  fields[lvl] points to
@@ -104,9 +107,18 @@ int    orc_evolve_states(const orc_desc *d, double *states, int64_t n,
 double orc_rplus(double a);
 double orc_risco(double a);
 
+/* ---- thermal emissivities (rt.cl:28-170) ---- */
+double orc_log_K2it(double te);
+double orc_B_Planck(double nu, double te);
+double orc_Gaunt(double x, double y);
+double orc_L_j_ff(double m_adm, double nu, double te, double ne);
+double orc_L_j_syn(double m_adm, double nu, double te, double ne, double b, double cos_theta);
+
 /* ---- numerical spacetime (interp.cl, dyst.cl) ---- */
 double orc_interp(const orc_grid *g, const double q[4], int comp);
 void   orc_dyst_rhs(const orc_grid *g, const double s[8], double ds[8]);
+/* geodesic + thermal transfer on n_data = 8 + 2 n_freq reals (phys.cl:66-74) */
+void   orc_dyst_rhs_rt(const orc_desc *d, const orc_grid *g, const double *s, double *ds);
 void   orc_dyst_down(const orc_grid *g, const double q[4], const double u[4], double k[4]);
 void   orc_dyst_icond(const orc_desc *d, const double cam[4], int64_t ray, double s[8]);
 double orc_dyst_getdt(double dt);

@@ -36,7 +36,11 @@ class OrcDesc(ctypes.Structure):
         ("flow", ctypes.c_int),
         ("torus_n0", ctypes.c_double), ("torus_kappa", ctypes.c_double),
         ("torus_hr", ctypes.c_double),
+        ("m_adm", ctypes.c_double), ("flow_te", ctypes.c_double), ("flow_b", ctypes.c_double),
     ]
+
+
+FLOW_THERMAL = 2
 
 
 class OrcGrid(ctypes.Structure):
@@ -103,6 +107,12 @@ def lib():
         L.orc_dyst_trace.argtypes = [P(OrcDesc), P(OrcGrid), pi64, i64, pd, pd,
                                      pi64, ctypes.c_int]
         L.orc_boosted_ks.argtypes = [d, d, d, ctypes.c_int, pd, pd]
+        for name, n in (("orc_log_K2it", 1), ("orc_B_Planck", 2), ("orc_Gaunt", 2),
+                        ("orc_L_j_ff", 4), ("orc_L_j_syn", 6)):
+            fn = getattr(L, name)
+            fn.restype = d
+            fn.argtypes = [d] * n
+        L.orc_dyst_rhs_rt.argtypes = [P(OrcDesc), P(OrcGrid), pd, pd]
         _lib = L
     return _lib
 
@@ -139,6 +149,9 @@ def make_desc(cfg):
     d.torus_n0 = cfg.get("torus_n0", 1.0)
     d.torus_kappa = cfg.get("torus_kappa", 1.0)
     d.torus_hr = cfg.get("torus_hr", 0.3)
+    d.m_adm = cfg.get("m_adm", 4.3e6)
+    d.flow_te = cfg.get("flow_te", 1e12)
+    d.flow_b = cfg.get("flow_b", 0.0)
     return d
 
 
@@ -292,14 +305,39 @@ def dyst_rhs(grid, s):
     return ds
 
 
+def _dyst_desc(cfg):
+    """Numerical renders carry the thermal flow when they have frequencies."""
+    if cfg.get("nu") and "flow" not in cfg:
+        cfg = dict(cfg, flow=FLOW_THERMAL)
+    return make_desc(cfg)
+
+
+def dyst_rhs_rt(cfg, grid, s):
+    """Geodesic and thermal-transfer RHS at state s (8 + 2 n_freq)."""
+    d = _dyst_desc(cfg)
+    s = np.ascontiguousarray(s, dtype=np.float64)
+    ds = np.zeros(8 + 2 * d.n_freq)
+    lib().orc_dyst_rhs_rt(ctypes.byref(d), ctypes.byref(grid.g), _p(s), _p(ds))
+    return ds
+
+
 def dyst_trace(cfg, grid, rays, nthreads=0):
     L = lib()
-    d = make_desc(cfg)
+    d = _dyst_desc(cfg)
     rays = np.ascontiguousarray(rays, dtype=np.int64)
     n = rays.size
-    out = np.zeros((n, 8))
+    out = np.zeros((n, n_data(cfg)))
     info = np.zeros(n)
     steps = np.zeros(n, dtype=np.int64)
-    L.orc_dyst_trace(ctypes.byref(d), ctypes.byref(grid.g), _pi(rays), n, _p(out),
-                     _p(info), _pi(steps), nthreads)
+    rc = L.orc_dyst_trace(ctypes.byref(d), ctypes.byref(grid.g), _pi(rays), n, _p(out),
+                          _p(info), _pi(steps), nthreads)
+    if rc != 0:
+        raise ValueError("oracle rejected the configuration")
     return out, info, steps
+
+
+def emissivities():
+    """The rt.cl emissivity functions of the oracle, by name."""
+    L = lib()
+    return {"log_K2it": L.orc_log_K2it, "B_Planck": L.orc_B_Planck, "Gaunt": L.orc_Gaunt,
+            "L_j_ff": L.orc_L_j_ff, "L_j_syn": L.orc_L_j_syn}

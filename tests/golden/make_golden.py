@@ -14,6 +14,10 @@ unmodified and records:
                           du^mu/dl = -Gamma^mu_ab u^a u^b with the tool's
                           Christoffels (boost 0, i.e. plain Kerr-Schild).
 
+It also checks, writing nothing, that the log K_2 table the library
+generates (gray_b200/csrc/make_logk2.py) holds the same numbers as the
+table of sim-org/rt.cl:51-67.
+
 Run from the repository root:
     python tests/golden/make_golden.py [path/to/reference/tools]
 The fixtures are committed; the tests never need the reference at run time.
@@ -117,6 +121,19 @@ def main():
         json.dump({"source": "classical RK4 on -Gamma u u from tools/boosted_ks.py",
                    "rays": rays}, f, indent=1)
     print("wrote", len(cases), "field cases and", len(rays), "rays")
+    check_logk2(os.path.join(os.path.dirname(os.path.abspath(tools)), "sim-org", "rt.cl"))
+
+
+def check_logk2(rt_cl):
+    import re
+    sys.path.insert(0, os.path.join(HERE, "..", "..", "gray_b200", "csrc"))
+    import make_logk2  # noqa: E402
+    src = open(rt_cl).read()
+    body = re.search(r"log_K2it_tab\[\]\s*=\s*\{(.*?)\}", src, re.S).group(1)
+    ref = np.array([float(x) for x in body.split(",")])
+    ours = np.array([float(make_logk2.fmt(x)) for x in make_logk2.values()])
+    assert np.array_equal(ref, ours), np.max(np.abs(ref - ours))
+    print("log K_2 table: %d values identical to %s" % (ref.size, "sim-org/rt.cl"))
 
 
 if __name__ == "__main__":
