@@ -16,8 +16,8 @@ LIB_PATH = os.path.join(HERE, "lib", "libgray_cuda.so")
 MAX_FREQ = 8
 ABI_VERSION = 2  # GRAY_ABI_VERSION of include/gray_cuda.h
 
-OK, EINVAL, ENOMEM, ECUDA, ENODEV, EBUDGET, ETIMEOUT, ENOTFOUND, ESTATE, ESIZE = (
-    0, -1, -2, -3, -4, -5, -6, -7, -8, -9)
+OK, EINVAL, ENOMEM, ECUDA, ENODEV, EBUDGET, ETIMEOUT, ENOTFOUND, ESTATE, ESIZE, ESOURCE = (
+    0, -1, -2, -3, -4, -5, -6, -7, -8, -9, -10)
 PREC_FP64, PREC_MIXED = 0, 1
 ST_KERR, ST_NUMERICAL = 0, 1
 FLOW_NONE, FLOW_TORUS, FLOW_THERMAL = 0, 1, 2
@@ -34,6 +34,7 @@ EXPORTS = [
     "gray_load_spacetime", "gray_load_spacetime_interleaved",
     "gray_make_boosted_ks", "gray_swap_levels", "gray_measure_peak",
     "gray_run_mixed_noalloc", "gray_read_spacetime",
+    "gray_series_schedule", "gray_run_series",
     "gray_batch_create", "gray_batch_destroy", "gray_batch_run", "gray_batch_steps",
     "gray_plan", "gray_set_plan", "gray_get_plan",
     "gray_serve_clock", "gray_serve_start", "gray_serve_submit", "gray_serve_poll",
@@ -102,6 +103,16 @@ class GridDesc(ctypes.Structure):
         ("box", ctypes.c_float * 8),
         ("bug_gzz", ctypes.c_int32), ("physics", ctypes.c_int32),
     ]
+
+
+LOAD_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
+                           ctypes.POINTER(ctypes.c_float))
+DUMP_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64)
+
+
+class SnapshotSource(ctypes.Structure):
+    _fields_ = [("n_times", ctypes.c_uint64), ("times", ctypes.POINTER(ctypes.c_double)),
+                ("user", ctypes.c_void_p), ("load", LOAD_FN)]
 
 
 # Reference defaults (sim/gray.opts, sim/Kerr.opts, sim/infcam.opts,
@@ -196,6 +207,9 @@ def lib():
         L.gray_serve_cancel.argtypes = [vp, u64]
         L.gray_serve_get_stats.argtypes = [vp, P(ServeStats)]
         L.gray_serve_stop.argtypes = [vp, i]
+        L.gray_series_schedule.argtypes = [P(d), u64, d, d, u64, i, P(ctypes.c_int64)]
+        L.gray_run_series.argtypes = [vp, i, P(GridDesc), P(SnapshotSource), i, DUMP_FN,
+                                      P(d), P(u64)]
         if L.gray_abi_version() != ABI_VERSION:
             raise RuntimeError("libgray_cuda.so has ABI %d, this module expects %d; rebuild"
                                % (L.gray_abi_version(), ABI_VERSION))
@@ -289,10 +303,64 @@ class Render:
         _ck(lib().gray_gather_steps(self.ctx.h, self.id, ctypes.byref(v)), "gray_gather_steps")
         return v.value
 
+    def run_series(self, grid, times, load, fast_light=False, after_dump=None):
+        """icond + every dump interval across a snapshot series
+        (gray_run_series).  load(k) returns snapshot k as nz*ny*nx*51 floats
+        (interleaved, or [z][y][x][51]); after_dump(i), if given, runs after
+        interval i.  Returns (device ns, number of load calls)."""
+        times = np.ascontiguousarray(times, dtype=np.float64)
+        npts = grid.nx * grid.ny * grid.nz
+        err = []
+
+        def _load(user, k, fields):
+            try:
+                a = np.ascontiguousarray(load(int(k)), dtype=np.float32).reshape(-1)
+                if a.size != npts * 51:
+                    raise ValueError("snapshot %d has %d floats, want %d" % (k, a.size, npts * 51))
+                ctypes.memmove(fields, a.ctypes.data, a.nbytes)
+                return 0
+            except Exception as e:  # reported after the call returns
+                err.append(e)
+                return 1
+
+        def _dump(user, i):
+            try:
+                after_dump(int(i))
+                return 0
+            except Exception as e:
+                err.append(e)
+                return 1
+
+        load_cb = LOAD_FN(_load)
+        dump_cb = DUMP_FN(_dump) if after_dump else DUMP_FN()
+        src = SnapshotSource(times.size, times.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                             None, load_cb)
+        ns = ctypes.c_double(0.0)
+        loads = ctypes.c_uint64(0)
+        st = lib().gray_run_series(self.ctx.h, self.id, ctypes.byref(grid), ctypes.byref(src),
+                                   int(bool(fast_light)), dump_cb, ctypes.byref(ns),
+                                   ctypes.byref(loads))
+        if err:
+            raise err[0]
+        _ck(st, "gray_run_series")
+        return ns.value, loads.value
+
     def close(self):
         if self.id:
             lib().gray_render_destroy(self.ctx.h, self.id)
             self.id = 0
+
+
+def series_schedule(times, t_init, dt_dump, n_dump, fast_light=False):
+    """The snapshot pair of each dump interval (gray_series_schedule)."""
+    times = np.ascontiguousarray(times, dtype=np.float64)
+    pairs = np.zeros(max(int(n_dump), 1), dtype=np.int64)
+    _ck(lib().gray_series_schedule(times.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                   times.size, float(t_init), float(dt_dump), int(n_dump),
+                                   int(bool(fast_light)),
+                                   pairs.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))),
+        "gray_series_schedule")
+    return pairs[:int(n_dump)]
 
 
 class Batch:

@@ -301,6 +301,54 @@ int gray_swap_levels(gray_ctx *ctx);
  * (nz*ny*nx*51*4 bytes): inspection of a loaded or generated grid. */
 int gray_read_spacetime(gray_ctx *ctx, int level, float *fields, size_t bytes);
 
+/* ---- time series of snapshots (sim-org/gray.c:147-294) --------------- */
+
+/* The snapshots of a dynamic spacetime: what the reference lists from the
+ * groups of its HDF5 file (io.c:150-230) and reads one at a time
+ * (load_snapshot, io.c:302-533).  load() fills `fields` -- nz*ny*nx*51
+ * floats, interleaved [z][y][x][51] in the field order of
+ * gray_load_spacetime -- with snapshot k and returns 0, or nonzero on
+ * failure.  It is called on the thread that called gray_run_series. */
+typedef struct gray_snapshot_source {
+	uint64_t      n_times;  /* snapshots available (>= 1)                   */
+	const double *times;    /* their times, strictly increasing             */
+	void         *user;
+	int         (*load)(void *user, uint64_t k, float *fields);
+} gray_snapshot_source;
+
+/* The snapshot pair (k, k+1) each dump interval integrates on, chosen as
+ * sim-org/gray.c:41-57 and 183-293 choose it: first the pair bracketing
+ * t_init, then, after each interval whose end time leaves [t_k, t_k+1],
+ * the pair bracketing that time.  pairs[i] is the pair of interval i + 1
+ * (from t_init + i dt_dump to t_init + (i+1) dt_dump).  With fast_light
+ * (param.opts enable_fast_light) or a single snapshot the spacetime is
+ * frozen: every entry is the snapshot bracketing t_init (0 for a single
+ * one) and the run interpolates in space only.  GRAY_EINVAL where the
+ * reference stops: t_init or the final time outside the series
+ * (sim-org/gray.c:193-205), times not increasing.  Host code only. */
+int gray_series_schedule(const double *times, uint64_t n_times, double t_init,
+                         double dt_dump, uint64_t n_dump, int fast_light,
+                         int64_t *pairs);
+
+/* Replaces the dynamic-spacetime loop of sim-org/gray.c:147-294 for a
+ * numerical render: icond at t_init, then its n_dump intervals, each on
+ * the snapshot pair of gray_series_schedule, with the level times of that
+ * pair.  `grid` gives the shape, spatial box and flags (its box times are
+ * ignored).  Snapshots stream: while an interval runs, the snapshot the
+ * next one needs is read (src->load) and copied to the device into a third
+ * level, and a pair that moves by one snapshot keeps the level it shares
+ * (copy_snapshot, io.c:279-300, becomes a relabelling).  after_dump
+ * (nullable) is called as after_dump(src->user, i) after interval
+ * i = 1..n_dump with the render's state readable, where the reference
+ * dumps (sim-org/gray.c:255); nonzero stops the run with
+ * GRAY_ESOURCE, as does a failing load().  *loads (nullable) receives the
+ * number of load() calls, *ns the elapsed device time.  The grid keeps the
+ * last pair as levels 0 and 1.  GRAY_ESTATE while the server runs. */
+int gray_run_series(gray_ctx *ctx, int render, const gray_grid_desc *grid,
+                    const gray_snapshot_source *src, int fast_light,
+                    int (*after_dump)(void *user, uint64_t i), double *ns,
+                    uint64_t *loads);
+
 /* ---- allocation-free entry point ----------------------------------- */
 
 /* No counterpart in the reference.  For callers that cannot call

@@ -12,6 +12,7 @@
 
 #include <limits.h>
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
 #include <omp.h>
@@ -1119,4 +1120,118 @@ orc_boosted_ks(double m, double a, double v, int axis, const double q[4], double
 	for(int i = 0; i < 4; ++i)
 		for(int j = i; j < 4; ++j)
 			out[k++] = gd[i][j];
+}
+
+/* ------------------------------------------------------------------------ */
+/* Snapshot series ("slow light", sim-org/gray.c:147-294)                    */
+/* ------------------------------------------------------------------------ */
+
+/* sim-org/gray.c:41-57 */
+static int64_t
+series_find(const double *times, int64_t n, double t)
+{
+	for(int64_t k = 0; k + 1 < n; ++k)
+		if(t >= times[k] && t <= times[k + 1])
+			return k;
+	return -1;
+}
+
+int
+orc_series_schedule(const double *times, int64_t n, double t_init, double dt_dump,
+                    int64_t n_dump, int fast_light, int64_t *first, int64_t *pairs)
+{
+	int64_t snap;
+	int frozen = n == 1 || fast_light;
+	if(n < 1)
+		return -1;
+	for(int64_t k = 1; k < n; ++k)
+		if(!(times[k] > times[k - 1]))
+			return -1;
+	if(n == 1)
+		snap = 0;                             /* gray.c:188-191 */
+	else if(fast_light)
+		snap = series_find(times, n, t_init); /* gray.c:214 */
+	else {
+		double t_final = t_init + (0 + 1) * dt_dump * n_dump; /* gray.c:200 */
+		if(t_init < times[0] || t_init > times[n - 1] ||
+		   t_final < times[0] || t_final > times[n - 1])
+			return -1;
+		snap = series_find(times, n, t_init); /* gray.c:232 */
+	}
+	if(snap < 0)
+		return -1;
+	*first = snap;
+	for(int64_t i = 0; i < n_dump; ) {
+		double target;
+		pairs[i] = snap;
+		target = t_init + (double)(++i) * dt_dump;
+		if(!frozen && (target < times[snap] || target > times[snap + 1])) {
+			snap = series_find(times, n, target); /* gray.c:267-270 */
+			if(snap < 0)
+				return -1;
+		}
+	}
+	return 0;
+}
+
+static void
+series_grid(const orc_grid *tmpl, const float *const *snaps, const double *times,
+            int64_t k, int frozen, orc_grid *g)
+{
+	*g = *tmpl;
+	g->fields[0] = snaps[k];
+	g->fields[1] = frozen ? snaps[k] : snaps[k + 1];
+	g->box[0] = frozen ? 0.0f : (float)times[k];     /* gray.c:225-226, 237-238 */
+	g->box[4] = frozen ? 0.0f : (float)times[k + 1];
+}
+
+int
+orc_dyst_series_trace(const orc_desc *d, const orc_grid *tmpl, const float *const *snaps,
+                      const double *times, int64_t n_times, int fast_light,
+                      const int64_t *rays, int64_t n, double *out, double *info,
+                      int64_t *steps, int nthreads)
+{
+	double cam[4];
+	const int nd = 8 + 2 * d->n_freq;
+	const int frozen = n_times == 1 || fast_light;
+	int64_t first, *pairs;
+	if(d->n_freq < 0 || d->n_freq > ORC_MAX_FREQ || d->n_sub <= 0)
+		return -1;
+	pairs = (int64_t *)malloc(sizeof(int64_t) * (d->n_dump ? d->n_dump : 1));
+	if(!pairs)
+		return -1;
+	if(orc_series_schedule(times, n_times, d->t_init, d->dt_dump, d->n_dump, fast_light,
+	                       &first, pairs)) {
+		free(pairs);
+		return -1;
+	}
+	orc_camera(d, cam);
+#ifdef _OPENMP
+	if(nthreads <= 0)
+		nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+#endif
+	for(int64_t j = 0; j < n; ++j) {
+		double *s = out + j * nd;
+		int64_t st = 0, k = first;
+		orc_grid g;
+		orc_dyst_icond(d, cam, rays[j], s);
+		for(int i = 0; i < 2 * d->n_freq; ++i)
+			s[8 + i] = 0.0;
+		for(int64_t i = 0; i < d->n_dump; ) {
+			k = pairs[i];
+			series_grid(tmpl, snaps, times, k, frozen, &g);
+			double t      = d->t_init + (double)i * d->dt_dump;
+			double target = d->t_init + (double)(++i) * d->dt_dump;
+			st += orc_dyst_evolve_ray(d, &g, s, target - t, d->n_sub);
+		}
+		series_grid(tmpl, snaps, times, k, frozen, &g);
+		steps[j] = st;
+		double kd[4];
+		orc_dyst_down(&g, s, s + 4, kd);
+		info[j] = dot4(kd, s + 4);
+	}
+	(void)nthreads;
+	free(pairs);
+	return 0;
 }

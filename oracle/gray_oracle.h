@@ -124,6 +124,18 @@ void   orc_dyst_icond(const orc_desc *d, const double cam[4], int64_t ray, doubl
 double orc_dyst_getdt(double dt);
 int64_t orc_dyst_evolve_ray(const orc_desc *d, const orc_grid *g, double *s,
                             double dt, int64_t n_sub);
+/* sim-org/gray.c:41-57 + 183-293: the snapshot pair of t_init (*first)
+ * and of every dump interval (pairs[n_dump]); -1 where the reference stops */
+int    orc_series_schedule(const double *times, int64_t n_times, double t_init,
+                           double dt_dump, int64_t n_dump, int fast_light,
+                           int64_t *first, int64_t *pairs);
+/* the dyst trace across a snapshot series: g gives shape, box and flags;
+ * snaps[k] are interleaved [z][y][x][51] levels at times[k] */
+int    orc_dyst_series_trace(const orc_desc *d, const orc_grid *g,
+                             const float *const *snaps, const double *times,
+                             int64_t n_times, int fast_light, const int64_t *rays,
+                             int64_t n, double *out, double *info, int64_t *steps,
+                             int nthreads);
 int    orc_dyst_trace(const orc_desc *d, const orc_grid *g, const int64_t *rays,
                       int64_t n, double *out, double *info, int64_t *steps,
                       int nthreads);

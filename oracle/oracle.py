@@ -113,6 +113,12 @@ def lib():
             fn.restype = d
             fn.argtypes = [d] * n
         L.orc_dyst_rhs_rt.argtypes = [P(OrcDesc), P(OrcGrid), pd, pd]
+        L.orc_series_schedule.restype = ctypes.c_int
+        L.orc_series_schedule.argtypes = [pd, i64, d, d, i64, ctypes.c_int, pi64, pi64]
+        L.orc_dyst_series_trace.restype = ctypes.c_int
+        L.orc_dyst_series_trace.argtypes = [P(OrcDesc), P(OrcGrid), P(ctypes.c_void_p), pd,
+                                            i64, ctypes.c_int, pi64, i64, pd, pd, pi64,
+                                            ctypes.c_int]
         _lib = L
     return _lib
 
@@ -341,3 +347,42 @@ def emissivities():
     L = lib()
     return {"log_K2it": L.orc_log_K2it, "B_Planck": L.orc_B_Planck, "Gaunt": L.orc_Gaunt,
             "L_j_ff": L.orc_L_j_ff, "L_j_syn": L.orc_L_j_syn}
+
+
+def series_schedule(times, t_init, dt_dump, n_dump, fast_light=False):
+    """Snapshot pair of t_init and of each dump interval (sim-org/gray.c:41-57,
+    183-293), or None where the reference stops."""
+    t = np.ascontiguousarray(times, dtype=np.float64)
+    first = np.zeros(1, dtype=np.int64)
+    pairs = np.zeros(max(n_dump, 1), dtype=np.int64)
+    rc = lib().orc_series_schedule(_p(t), t.size, float(t_init), float(dt_dump), int(n_dump),
+                                   int(bool(fast_light)), _pi(first), _pi(pairs))
+    return None if rc else (int(first[0]), pairs[:n_dump].copy())
+
+
+def dyst_series_trace(cfg, snaps, times, lo, hi, rays, physics=False, bug_gzz=False,
+                      fast_light=False, nthreads=0):
+    """dyst trace across a snapshot series (snaps[k]: [nz][ny][nx][51] at times[k]);
+    every interval runs on the pair sim-org/gray.c chooses for it."""
+    L = lib()
+    d = _dyst_desc(cfg)
+    snaps = [np.ascontiguousarray(a, dtype=np.float32) for a in snaps]
+    nz, ny, nx, _ = snaps[0].shape
+    g = OrcGrid()
+    g.nx, g.ny, g.nz = nx, ny, nz
+    for i, v in enumerate([0.0, lo, lo, lo, 0.0, hi, hi, hi]):
+        g.box[i] = v
+    g.bug_gzz, g.physics = int(bug_gzz), int(physics)
+    ptrs = (ctypes.c_void_p * len(snaps))(*[a.ctypes.data for a in snaps])
+    t = np.ascontiguousarray(times, dtype=np.float64)
+    rays = np.ascontiguousarray(rays, dtype=np.int64)
+    n = rays.size
+    out = np.zeros((n, n_data(cfg)))
+    info = np.zeros(n)
+    steps = np.zeros(n, dtype=np.int64)
+    rc = L.orc_dyst_series_trace(ctypes.byref(d), ctypes.byref(g), ptrs, _p(t), t.size,
+                                 int(bool(fast_light)), _pi(rays), n, _p(out), _p(info),
+                                 _pi(steps), nthreads)
+    if rc != 0:
+        raise ValueError("oracle rejected the series")
+    return out, info, steps
