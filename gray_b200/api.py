@@ -23,13 +23,16 @@ ST_KERR, ST_NUMERICAL = 0, 1
 FLOW_NONE, FLOW_TORUS, FLOW_THERMAL = 0, 1, 2
 TERM_EPS, TERM_RPLUS = 0, 1
 LAYOUT_SOA, LAYOUT_AOS = 0, 1
+COORDS_SPH_KS, COORDS_BL = 0, 1
+COORDS_AS_WRITTEN = 1
 
 # Every symbol include/gray_cuda.h declares.
 EXPORTS = [
     "gray_strerror", "gray_abi_version", "gray_create", "gray_destroy",
     "gray_set_stream", "gray_sync", "gray_hbm_used", "gray_render_create",
     "gray_render_destroy", "gray_icond", "gray_evolve", "gray_run", "gray_evolve_all",
-    "gray_read_state", "gray_write_state", "gray_read_kdown", "gray_ray_steps",
+    "gray_read_state", "gray_write_state", "gray_read_kdown", "gray_read_coords",
+    "gray_ray_steps",
     "gray_gather_steps",
     "gray_load_spacetime", "gray_load_spacetime_interleaved",
     "gray_make_boosted_ks", "gray_swap_levels", "gray_measure_peak",
@@ -182,6 +185,7 @@ def lib():
         L.gray_read_state.argtypes = [vp, i, vp, sz, vp, sz, i]
         L.gray_write_state.argtypes = [vp, i, vp, sz, i]
         L.gray_read_kdown.argtypes = [vp, i, vp, sz]
+        L.gray_read_coords.argtypes = [vp, i, i, d, i, vp, sz]
         L.gray_ray_steps.argtypes = [vp, i, P(u64)]
         L.gray_gather_steps.argtypes = [vp, i, P(u64)]
         L.gray_load_spacetime.argtypes = [vp, P(GridDesc), P(ctypes.c_void_p), i]
@@ -292,6 +296,13 @@ class Render:
         k = np.empty((4, self.n_rays), dtype=np.float64)
         _ck(lib().gray_read_kdown(self.ctx.h, self.id, k.ctypes.data, k.nbytes), "gray_read_kdown")
         return k
+
+    def coords(self, system=COORDS_BL, r_match=10.0, flags=0):
+        """(8, n_rays): t, r, theta, phi, u^t, u^r, u^theta, u^phi (KS.cl:63-153)."""
+        out = np.empty((8, self.n_rays), dtype=np.float64)
+        _ck(lib().gray_read_coords(self.ctx.h, self.id, system, float(r_match), flags,
+                                   out.ctypes.data, out.nbytes), "gray_read_coords")
+        return out
 
     def steps(self):
         v = ctypes.c_uint64(0)

@@ -724,6 +724,40 @@ gray_read_kdown(gray_ctx *c, int id, double *k, size_t bytes)
 }
 
 extern "C" int
+gray_read_coords(gray_ctx *c, int id, int system, double r_match, int flags, double *out,
+                 size_t bytes)
+{
+	Render *r = find(c, id);
+	if(!r)
+		return GRAY_ENOTFOUND;
+	if(!r->has_state)
+		return GRAY_ESTATE;
+	if(!out || (system != GRAY_COORDS_SPH_KS && system != GRAY_COORDS_BL) ||
+	   (flags & ~GRAY_COORDS_AS_WRITTEN))
+		return GRAY_EINVAL;
+	if(r->p.spacetime != GRAY_ST_KERR)
+		return GRAY_EINVAL;
+	if(system == GRAY_COORDS_BL && !(std::isfinite(r_match) && r_match > r->p.rp))
+		return GRAY_EINVAL;
+	const size_t nr = (size_t)r->p.n_rays;
+	if(bytes != nr * 8 * sizeof(double))
+		return GRAY_ESIZE;
+	CK(cudaSetDevice(c->device));
+	void *tmp = nullptr;
+	int st = dalloc(c, &tmp, bytes);
+	if(st)
+		return st;
+	cudaError_t e = launch_coords64(r->p, r->d_data, (double *)tmp, system, r_match,
+	                                (flags & GRAY_COORDS_AS_WRITTEN) ? 1 : 0, c->stream);
+	if(e == cudaSuccess)
+		e = cudaMemcpyAsync(out, tmp, bytes, cudaMemcpyDeviceToHost, c->stream);
+	if(e == cudaSuccess)
+		e = cudaStreamSynchronize(c->stream);
+	dfree(c, tmp, bytes);
+	return from_cuda(e);
+}
+
+extern "C" int
 gray_ray_steps(gray_ctx *c, int id, uint64_t *steps)
 {
 	Render *r = find(c, id);

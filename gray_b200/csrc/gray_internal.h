@@ -81,6 +81,8 @@ cudaError_t launch_kdown64(const RenderParams &p, const double *data, double *k,
                            cudaStream_t st);
 cudaError_t launch_getuu64(const RenderParams &p, const double *data, double *info,
                            cudaStream_t st);
+cudaError_t launch_coords64(const RenderParams &p, const double *data, double *out,
+                            int system, double r_match, int as_written, cudaStream_t st);
 cudaError_t launch_transpose(const double *src, double *dst, long long n_rays,
                              int n_data, int to_aos, cudaStream_t st);
 

@@ -384,6 +384,81 @@ kdown64_kernel(const RenderParams p, const double *__restrict__ data,
 		k[c * n + g] = kk[c];
 }
 
+/* KS.cl:63-153 output coordinates, in the oracle's operation order.  The
+ * event of down()'s metric is x + i y = (r + i a) e^(i phi) sin(theta);
+ * KS.cl:68-69 and 130 use (r - i a), and KS.cl:148-151 put u^phi and u^t
+ * where u^r belongs: as_written reproduces both. */
+__device__ __forceinline__ void
+sph_ks64(const RenderParams &p, const double *q, int as_written, double *out)
+{
+	double r = sqrt(getrr64(p, q[1], q[2], q[3]));
+	double sa = as_written ? p.a : -p.a;
+	out[0] = q[0];
+	out[1] = r;
+	out[2] = acos(q[3] / r);
+	out[3] = atan2(fma(q[2], r, q[1] * sa), fma(q[1], r, -(q[2] * sa)));
+}
+
+__device__ __forceinline__ void
+sph_ks_u64(const RenderParams &p, const double *q, const double *u, int as_written,
+           double *out)
+{
+	const double aa = p.aa;
+	double RR = fma(q[1], q[1], q[2] * q[2]);
+	double zz = q[3] * q[3];
+	double kk = 0.5 * (RR + zz - aa);
+	double dd = sqrt(fma(kk, kk, aa * zz));
+	double rr = dd + kk;
+	double r  = sqrt(rr);
+	double den = 2.0 * r * dd;
+	double J1[4] = {0.0, rr * q[1] / den, rr * q[2] / den, (rr + aa) * q[3] / den};
+	double zr = q[3] / r, sq = sqrt(rr - zz);
+	double J2[4] = {0.0, zr * J1[1] / sq, zr * J1[2] / sq, (zr * J1[3] - 1.0) / sq};
+	double c = (as_written ? -p.a : p.a) / (rr + aa);
+	double J3[4] = {0.0, fma(c, J1[1], -q[2] / RR), fma(c, J1[2], q[1] / RR), c * J1[3]};
+	out[0] = u[0];
+	out[1] = fma(J1[3], u[3], fma(J1[2], u[2], J1[1] * u[1]));
+	out[2] = fma(J2[3], u[3], fma(J2[2], u[2], J2[1] * u[1]));
+	out[3] = fma(J3[3], u[3], fma(J3[2], u[2], J3[1] * u[1]));
+}
+
+/* system 0: spherical KS; 1: Boyer-Lindquist with t matched at r_match */
+__global__ void
+coords64_kernel(const RenderParams p, const double *__restrict__ data,
+                double *__restrict__ out, int system, double r_match, int as_written)
+{
+	const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	const long long n = p.n_rays;
+	if(g >= n)
+		return;
+	double s[8], x[4], v[4];
+#pragma unroll
+	for(int c = 0; c < 8; ++c)
+		s[c] = data[c * n + g];
+	const double *q = s, *u = s + 4;
+	sph_ks64(p, q, as_written, x);
+	sph_ks_u64(p, q, u, as_written, v);
+	if(system == 1) {
+		double h  = sqrt(1.0 - p.aa);
+		double rp = 1.0 + h, rm = 1.0 - h, r = x[1];
+		x[0] = x[0] + (rm * log((r - rm) / (r_match - rm)) -
+		               rp * log((r - rp) / (r_match - rp))) / h;
+		x[3] = x[3] + 0.5 * p.a * log((r - rm) / (r - rp)) / h;
+		double rr = getrr64(p, q[1], q[2], q[3]);
+		double rq = sqrt(rr);
+		double D  = rr - 2.0 * rq + p.aa;
+		double ut = as_written ? v[3] : v[1];
+		double up = as_written ? v[0] : v[1];
+		v[0] = v[0] - ut * 2.0 * rq / D;
+		v[3] = v[3] - up * p.a / D;
+	}
+#pragma unroll
+	for(int c = 0; c < 4; ++c) {
+		out[c * n + g] = x[c];
+		out[(4 + c) * n + g] = v[c];
+	}
+}
+
 __global__ void
 getuu64_kernel(const RenderParams p, const double *__restrict__ data,
                double *__restrict__ info)
@@ -474,6 +549,15 @@ cudaError_t
 launch_kdown64(const RenderParams &p, const double *data, double *k, cudaStream_t st)
 {
 	kdown64_kernel<<<blocks_for(p.n_rays, 128), 128, 0, st>>>(p, data, k);
+	return cudaGetLastError();
+}
+
+cudaError_t
+launch_coords64(const RenderParams &p, const double *data, double *out, int system,
+                double r_match, int as_written, cudaStream_t st)
+{
+	coords64_kernel<<<blocks_for(p.n_rays, 128), 128, 0, st>>>(p, data, out, system, r_match,
+	                                                           as_written);
 	return cudaGetLastError();
 }
 

@@ -170,6 +170,25 @@ int gray_write_state(gray_ctx *ctx, int render_id, const void *data,
  * n_rays * 4 doubles in SoA order. */
 int gray_read_kdown(gray_ctx *ctx, int render_id, double *k, size_t bytes);
 
+/* Output coordinates of an analytic render's state (KS.cl:63-153), n_rays
+ * * 8 doubles in SoA order: t, r, theta, phi, then u^t, u^r, u^theta,
+ * u^phi.  GRAY_COORDS_SPH_KS is getsphKS/getsphKSu; GRAY_COORDS_BL is
+ * getBL/getBLu with t_BL = t_KS at r_match (> r_+; the reference leaves
+ * r_match undefined) and phi matched at infinity.  Two lines of KS.cl
+ * disagree with the metric the path integrates (down(), KS.cl:91-114):
+ * phi is taken with (r - i a) where the metric's event is x + i y =
+ * (r + i a) e^(i phi) sin(theta) (KS.cl:68-69, 130), and getBLu multiplies
+ * u^phi and u^t where the change of coordinates has u^r (KS.cl:148-151).
+ * By default both follow the metric, so a null ray stays null in the
+ * Boyer-Lindquist metric; GRAY_COORDS_AS_WRITTEN reproduces the lines. */
+enum gray_coords {
+	GRAY_COORDS_SPH_KS = 0,
+	GRAY_COORDS_BL     = 1
+};
+#define GRAY_COORDS_AS_WRITTEN 1
+int gray_read_coords(gray_ctx *ctx, int render_id, int system, double r_match, int flags,
+                     double *out, size_t bytes);
+
 /* Accepted RK4 steps summed over the render's rays since the last icond. */
 int gray_ray_steps(gray_ctx *ctx, int render_id, uint64_t *steps);
 

@@ -48,6 +48,88 @@ orc_geteps(double a, const double q[4])
 	return sqrt(orc_getrr(a, q)) - orc_rplus(a);
 }
 
+/* KS.cl:63-153 output coordinates.  The Cartesian Kerr-Schild event of the
+ * metric of down() (l = (1, (r x + a y)/(r^2 + a^2), (r y - a x)/(r^2 + a^2),
+ * z/r)) is x + i y = (r + i a) e^(i phi) sin(theta), z = r cos(theta), so
+ * phi = arg((x + i y)(r - i a)).  KS.cl:68-69 takes arg((x + i y)(r + i a))
+ * (and KS.cl:130 the matching d phi), and KS.cl:148-151 multiply u^phi and
+ * u^t where the coordinate change has u^r: as_written = 1 reproduces those
+ * lines, 0 gives coordinates in which the metric is Kerr's in
+ * Boyer-Lindquist form. */
+
+/* KS.cl:63-71 getsphKS(): (t, r, theta, phi) */
+void
+orc_getsphKS(double a, const double q[4], int as_written, double out[4])
+{
+	double r = sqrt(orc_getrr(a, q));
+	double sa = as_written ? a : -a;
+	out[0] = q[0];
+	out[1] = r;
+	out[2] = acos(q[3] / r);
+	out[3] = atan2(fma(q[2], r, q[1] * sa), fma(q[1], r, -(q[2] * sa)));
+}
+
+/* KS.cl:73-89 getBL(): t matched to t_KS at r_match (a free parameter:
+ * the reference never defines it), phi matched at r = infinity */
+void
+orc_getBL(double a, double r_match, const double q[4], int as_written, double out[4])
+{
+	double s[4];
+	orc_getsphKS(a, q, as_written, s);
+	double h  = sqrt(1.0 - a * a);
+	double rp = 1.0 + h, rm = 1.0 - h, r = s[1];
+	out[0] = s[0] + (rm * log((r - rm) / (r_match - rm)) -
+	                 rp * log((r - rp) / (r_match - rp))) / h;
+	out[1] = s[1];
+	out[2] = s[2];
+	out[3] = s[3] + 0.5 * a * log((r - rm) / (r - rp)) / h;
+}
+
+/* KS.cl:116-133 getsphKSu(): the Jacobian rows dr, dtheta, dphi of the
+ * Cartesian KS position applied to u */
+void
+orc_getsphKSu(double a, const double q[4], const double u[4], int as_written, double out[4])
+{
+	double aa = a * a;
+	double RR = fma(q[1], q[1], q[2] * q[2]);
+	double zz = q[3] * q[3];
+	double kk = 0.5 * (RR + zz - aa);
+	double dd = sqrt(fma(kk, kk, aa * zz));
+	double rr = dd + kk;
+	double r  = sqrt(rr);
+	double den = 2.0 * r * dd;
+	double J1[4] = {0.0, rr * q[1] / den, rr * q[2] / den, (rr + aa) * q[3] / den};
+	double zr = q[3] / r, sq = sqrt(rr - zz);
+	double J2[4] = {0.0, zr * J1[1] / sq, zr * J1[2] / sq, (zr * J1[3] - 1.0) / sq};
+	double c = (as_written ? -a : a) / (rr + aa);
+	double J3[4] = {0.0, fma(c, J1[1], -q[2] / RR), fma(c, J1[2], q[1] / RR), c * J1[3]};
+	out[0] = u[0];
+	out[1] = fma(J1[3], u[3], fma(J1[2], u[2], J1[1] * u[1]));
+	out[2] = fma(J2[3], u[3], fma(J2[2], u[2], J2[1] * u[1]));
+	out[3] = fma(J3[3], u[3], fma(J3[2], u[2], J3[1] * u[1]));
+}
+
+/* KS.cl:135-153 getBLu(): dt_BL = dt - 2r/Delta dr, dphi_BL = dphi -
+ * a/Delta dr */
+void
+orc_getBLu(double a, const double q[4], const double u[4], int as_written, double out[4])
+{
+	double v[4];
+	orc_getsphKSu(a, q, u, as_written, v);
+	double aa = a * a;
+	double zz = q[3] * q[3];
+	double kk = 0.5 * (fma(q[1], q[1], fma(q[2], q[2], zz)) - aa);
+	double rr = sqrt(fma(kk, kk, aa * zz)) + kk;
+	double r  = sqrt(rr);
+	double D  = rr - 2.0 * r + aa;
+	double ut = as_written ? v[3] : v[1]; /* multiplies 2r / Delta */
+	double up = as_written ? v[0] : v[1]; /* multiplies a / Delta  */
+	out[0] = v[0] - ut * 2.0 * r / D;
+	out[1] = v[1];
+	out[2] = v[2];
+	out[3] = v[3] - up * a / D;
+}
+
 /* The KS scalar f and null covector l_mu = (1, lx, ly, lz), computed with
  * the same operation sequence as the head of orc_ks_rhs() (KS.cl:282-333),
  * so the reuse inside the RHS and the stand-alone down() agree bitwise. */

@@ -74,6 +74,16 @@ double orc_getrr(double a, const double q[4]);
 double orc_geteps(double a, const double q[4]);
 void   orc_down(double a, const double q[4], const double u[4], double k[4]);
 double orc_getuu(double a, const double s[8]);
+/* KS.cl:63-153 output coordinates: spherical Kerr-Schild and
+ * Boyer-Lindquist events and vectors; r_match is where t_BL = t_KS;
+ * as_written = 1 reproduces KS.cl's phi convention and getBLu terms */
+void   orc_getsphKS(double a, const double q[4], int as_written, double out[4]);
+void   orc_getBL(double a, double r_match, const double q[4], int as_written,
+                 double out[4]);
+void   orc_getsphKSu(double a, const double q[4], const double u[4], int as_written,
+                     double out[4]);
+void   orc_getBLu(double a, const double q[4], const double u[4], int as_written,
+                  double out[4]);
 void   orc_ks_rhs(double a, const double s[8], double ds[8]);
 
 /* Per-render camera constants computed once on the host:

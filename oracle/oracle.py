@@ -113,6 +113,10 @@ def lib():
             fn.restype = d
             fn.argtypes = [d] * n
         L.orc_dyst_rhs_rt.argtypes = [P(OrcDesc), P(OrcGrid), pd, pd]
+        L.orc_getsphKS.argtypes = [d, pd, ctypes.c_int, pd]
+        L.orc_getBL.argtypes = [d, d, pd, ctypes.c_int, pd]
+        L.orc_getsphKSu.argtypes = [d, pd, pd, ctypes.c_int, pd]
+        L.orc_getBLu.argtypes = [d, pd, pd, ctypes.c_int, pd]
         L.orc_series_schedule.restype = ctypes.c_int
         L.orc_series_schedule.argtypes = [pd, i64, d, d, i64, ctypes.c_int, pi64, pi64]
         L.orc_dyst_series_trace.restype = ctypes.c_int
@@ -386,3 +390,21 @@ def dyst_series_trace(cfg, snaps, times, lo, hi, rays, physics=False, bug_gzz=Fa
     if rc != 0:
         raise ValueError("oracle rejected the series")
     return out, info, steps
+
+
+def coords(a, s, system="bl", r_match=10.0, as_written=False):
+    """Output coordinates of one 8-component KS state (KS.cl:63-153):
+    (t, r, theta, phi, u^t, u^r, u^theta, u^phi) in spherical KS ("sph")
+    or Boyer-Lindquist ("bl")."""
+    L = lib()
+    s = np.ascontiguousarray(s, dtype=np.float64)
+    q, u = np.ascontiguousarray(s[:4]), np.ascontiguousarray(s[4:8])
+    x, v = np.zeros(4), np.zeros(4)
+    w = int(bool(as_written))
+    if system == "sph":
+        L.orc_getsphKS(a, _p(q), w, _p(x))
+        L.orc_getsphKSu(a, _p(q), _p(u), w, _p(v))
+    else:
+        L.orc_getBL(a, r_match, _p(q), w, _p(x))
+        L.orc_getBLu(a, _p(q), _p(u), w, _p(v))
+    return np.r_[x, v]
