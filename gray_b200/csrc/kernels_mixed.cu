@@ -140,8 +140,8 @@ template <> struct Lanes<F2> { static constexpr int N = 2; };
 
 template <typename V, int NF>
 struct RC {
-	V a, aa, risco, kappa, n0_rp15, ihr2, torus;
-	V nupow[NF > 0 ? NF : 1], nuinv2[NF > 0 ? NF : 1];
+	V a, aa, risco, kappa, n0t, ihr2;
+	V lgnupow[NF > 0 ? NF : 1], nuinv2[NF > 0 ? NF : 1];
 };
 
 template <typename V, int NF>
@@ -152,12 +152,12 @@ load_rc(RC<V, NF> &rc, int k, const MixedRender &c)
 	setl(rc.aa, k, c.aa);
 	setl(rc.risco, k, c.risco);
 	setl(rc.kappa, k, c.kappa);
-	setl(rc.n0_rp15, k, c.n0_rp15);
+	/* the density scale, zero without the torus flow */
+	setl(rc.n0t, k, c.flow == GRAY_FLOW_TORUS ? c.n0_rp15 : 0.0f);
 	setl(rc.ihr2, k, c.ihr2_log2e);
-	setl(rc.torus, k, c.flow == GRAY_FLOW_TORUS ? 1.0f : 0.0f);
 #pragma unroll
 	for(int i = 0; i < NF; ++i) {
-		setl(rc.nupow[i], k, c.nupow[i]);
+		setl(rc.lgnupow[i], k, log2f(c.nupow[i])); /* nu_i^-0.7 as a power of 2 */
 		setl(rc.nuinv2[i], k, c.nuinv2[i]);
 	}
 }
@@ -303,15 +303,15 @@ torus_rt(const RC<V, NF> &c, const V *s, const Aux<V> &x, V *ds)
 	V sh = selv(ok, shift, one);
 	/* n0 (r_+/r)^1.5 exp(-z^2 / (2 (h r)^2)) */
 	V e = ex2v(-((q3 * q3) * ((x.ir * x.ir) * c.ihr2)));
-	V n = selv(ok, (c.n0_rp15 * c.torus) * ((x.ir * irs) * e), zero);
-	V ish  = rcpv(sh);
-	/* -j(nu) / shift^2 with j = n nu_i^-0.7 shift^-0.7, factored once */
-	V mjis2 = -((n * ex2v(bc<V>(-0.7f) * lg2v(sh))) * (ish * ish));
-	V mtfac = -((c.kappa * n) * ish);
+	V n = selv(ok, c.n0t * ((x.ir * irs) * e), zero);
+	/* -j(nu) / shift^2 = -n nu_i^-0.7 shift^-2.7: one power of the shift
+	 * for all frequencies, nu_i^-0.7 e^-tau_i as one power of 2 each */
+	V mjis2 = -(n * ex2v(bc<V>(-2.7f) * lg2v(sh)));
+	V mtfac = -((c.kappa * n) * rcpv(sh));
 	const V mlog2e = bc<V>(-1.4426950408889634f);
 #pragma unroll
 	for(int i = 0; i < NF; ++i) {
-		ds[8 + i]      = (mjis2 * c.nupow[i]) * ex2v(s[8 + NF + i] * mlog2e);
+		ds[8 + i]      = mjis2 * ex2v(fmav(s[8 + NF + i], mlog2e, c.lgnupow[i]));
 		ds[8 + NF + i] = mtfac * c.nuinv2[i];
 	}
 }
