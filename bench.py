@@ -57,7 +57,7 @@ TRAFFIC = {}
 # Host-to-device bytes of one render through the C ABI: the render's table
 # entry (sizeof(MixedRender) in gray_b200/csrc/mixed_table.h); the camera
 # initial conditions are generated on the device.
-H2D_BYTES_PER_RENDER = 336
+H2D_BYTES_PER_RENDER = 392
 
 
 def parse():

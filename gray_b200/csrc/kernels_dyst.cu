@@ -87,6 +87,102 @@ struct DystConst {
 	float B[3], iA[3];
 };
 
+/* ------------------------------------------------ thermal transfer island */
+
+/* 1/b to ~1e-14 relative: the FP32 approximate reciprocal refined by one
+ * FP64 Newton step (b within the FP32 normal range) */
+__device__ __forceinline__ double
+rcp64(double b)
+{
+	const double r = (double)rcp_a((float)b);
+	return fma(r, fma(-b, r, 1.0), r);
+}
+
+/* e^x for |x| within the FP32 range, ~1e-7 relative */
+__device__ __forceinline__ float
+exp_f(float x)
+{
+	return ex2_a(x * 1.4426950408889634f);
+}
+
+/* rt.cl:80-198 for the mixed kernel: the magnitudes (1e-47 .. 1e+39 in CGS)
+ * stay FP64, the special functions of O(1) arguments (exp, log, cbrt,
+ * sqrt) take the FP32 approximate instructions, and everything that
+ * depends only on the render is a ThermalFast constant.  Same formulas and
+ * branches as the FP64 kernels; agreement to ~1e-6 relative. */
+template <int NF>
+__device__ __forceinline__ void
+rt_rhs_fast(const ThermalFast &t, const double *nu_hz, const double *k, double ne,
+            const double *tau, double *dI, double *dtau)
+{
+	const double EPS = GRAY_EPSILON;
+	const double shift = -k[0];
+	const float bkcos = (float)(k[3] * t.b) * rcp_a((float)(shift * t.b + EPS));
+	const double ish2 = rcp64(fma(shift, shift, EPS));
+	/* synchrotron frequency: nu_s = knus sin(theta), zero along the field */
+	double nus = 0.0, inus = 0.0;
+	const bool syn = t.syn && bkcos > -1.0f && bkcos < 1.0f;
+	if(syn) {
+		nus = t.knus * (double)sqrt_a(fmaf(-bkcos, bkcos, 1.0f));
+		inus = rcp64(nus + EPS);
+	}
+	const double ne2 = ne * ne;
+#pragma unroll
+	for(int i = 0; i < NF; ++i) {
+		const double nu = nu_hz[i] * shift;
+		/* rt.cl:80-93 */
+		const double f2 = nu * t.kf2;
+		double B;
+		if(f2 > 1e-5) {
+			double em1;
+			if(f2 < 0.3) /* e^f2 - 1 by its series: no cancellation */
+				em1 = f2 * fma(f2, fma(f2, fma(f2, fma(f2, fma(f2, fma(f2,
+				      1.0 / 5040, 1.0 / 720), 1.0 / 120), 1.0 / 24), 1.0 / 6), 0.5), 1.0);
+			else if(f2 < 80.0)
+				em1 = (double)exp_f((float)f2) - 1.0;
+			else
+				em1 = exp(f2);
+			B = t.kB * (nu * nu) * nu / em1;
+		} else {
+			B = t.kB2 * (nu * nu) * rcp64(fma(f2, fma(f2, 1.0 / 6, 0.5), 1.0));
+		}
+		/* rt.cl:95-143 bremsstrahlung */
+		const double y = nu * t.ky;
+		double Lff = 0.0;
+		if(y < 80.0) {
+			const float yf = (float)(y + EPS);
+			const float sy = sqrt_a((float)y);
+			double G;
+			if(t.xg > 1.0)
+				G = y > 1.0 ? t.g1 / (double)sy
+				            : t.g2 * (t.g3 - 0.6931471805599453 * (double)lg2_a(yf));
+			else if(t.xg * y > 1.0)
+				G = t.g5 * rcp64(t.sxg * (double)sy);
+			else if(y > t.sxg)
+				G = 1.0;
+			else {
+				G = t.g2 * (t.g4 + 0.6931471805599453 *
+				                      (double)(lg2_a((float)t.sxg) - lg2_a(yf)));
+				G = G > EPS ? G : EPS;
+			}
+			Lff = (t.kff * ne2) * G * rcp64(fma(t.sqte, (double)exp_f((float)y), EPS));
+		}
+		/* rt.cl:145-170 synchrotron */
+		double Lsyn = 0.0;
+		if(syn) {
+			double x = nu * inus;
+			x = x < 1e30 ? x : 1e30; /* e^-cbrt(x) is 0 long before */
+			const float xf = (float)x;
+			const float cx = ex2_a(0.33333334f * lg2_a(xf));
+			const double xx = (double)sqrt_a(xf) + 1.88774862536 * (double)sqrt_a(cx);
+			Lsyn = t.ksyn * (xx * xx) * (double)exp_f(-cx) * (ne * nus);
+		}
+		const double L = Lsyn + Lff;
+		dI[i]   = -L * (double)exp_f(-(float)tau[i]) * ish2;
+		dtau[i] = -L * shift * rcp64(B + EPS);
+	}
+}
+
 __device__ __forceinline__ bool
 inside32(const GridParams &g, const float *q)
 {
@@ -305,7 +401,6 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 		float k[ND], t[ND], sum[ND];
 		cnt_in += (!g.physics || inside32(g, hi)) ? 1 : 0;
 		if constexpr(NF > 0) {
-			const thermal::Flow fl = {c->nu_hz, c->m_adm, c->flow_te, c->flow_b, &c->th};
 			const double hsd = (double)dh * dtnd;
 			double trt[NR], srt[NR], krt[NR];
 #pragma unroll
@@ -319,7 +414,7 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 				float kn[5];
 				dyst_rhs32<true>(g, dc, t, k, kn);
 				const double kd[4] = {kn[0], kn[1], kn[2], kn[3]};
-				thermal::rt_rhs<NF>(fl, kd, (double)kn[4], trt + NF, krt, krt + NF);
+				rt_rhs_fast<NF>(c->tf, c->nu_hz, kd, (double)kn[4], trt + NF, krt, krt + NF);
 				const float wg = (st == 1 || st == 2) ? 2.0f : 1.0f;
 				const float cg = st < 2 ? hh : hs;
 				const double wd = wg, cd = st < 2 ? 0.5 * hsd : hsd;

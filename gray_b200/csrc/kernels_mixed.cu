@@ -26,6 +26,7 @@
 #include <climits>
 
 #include "gray_internal.h"
+#include "logk2_table.h"
 #include "mixed_table.h"
 
 namespace {
@@ -697,6 +698,43 @@ mixed_occupancy(int n_freq, const MixedLaunch &cfg, int *blocks_per_sm)
 #undef OCC
 }
 
+/* Per-render constants of the thermal emissivities (rt.cl:80-170), FP64 on
+ * the host; log K_2(1/te) exactly as rt.cl:70-78 and 166-167 compute it. */
+static void
+thermal_fast(const RenderParams &p, ThermalFast *t)
+{
+	const double c = 2.99792458e+10, h = 6.62606957e-27, G = 6.67384800e-08,
+	             Ry = 2.17987197e-11, e = 4.80320425e-10, me = 9.10938291e-28,
+	             msun = 1.98910000e+33, pi = 3.14159265358979323846,
+	             sqrt2 = 1.41421356237309504880, eps = GRAY_EPSILON;
+	const double te = p.flow_te, b = p.flow_b;
+	static const double LOGK2[GRAY_LOGK2_N] = {GRAY_LOGK2_VALUES};
+	t->kf2 = h / (me * c) / c / (te + eps);
+	t->kB = 2.0 * h / (c * c);
+	t->kB2 = 2.0 * h / (c * c) / t->kf2;
+	t->ky = h / (me * c * c) / te;
+	t->xg = me * c * c / Ry * te;
+	t->sxg = sqrt(t->xg);
+	t->g1 = p.th.g1; t->g2 = p.th.g2; t->g3 = p.th.g3; t->g4 = p.th.g4; t->g5 = p.th.g5;
+	t->kff = p.m_adm * p.th.ff_f * p.th.ff_f;
+	t->sqte = sqrt(te);
+	t->knus = te * te * b * (e / (9 * pi * me * c));
+	double log_K2 = 0.0;
+	if(te > 1e+2) {
+		log_K2 = log(2 * te * te - 0.5);
+	} else if(te > 1e-1) {
+		const double hh = log(te / 1e-1) * p.th.lk_scale;
+		int i = (int)hh;
+		if(i > 59)
+			i = 59;
+		const double d = hh - i;
+		log_K2 = (1 - d) * LOGK2[i] + d * LOGK2[i + 1];
+	}
+	t->ksyn = p.m_adm * ((G * msun / (c * c)) * (sqrt2 * pi * e * e / (3 * c))) * exp(-log_K2);
+	t->b = b;
+	t->syn = te > 1e-1 && b != 0.0;
+}
+
 void
 fill_mixed_render(const RenderParams &p, double *data, double *info, double t_init,
                   double dt_dump, long long n_dump, long long n_sub, MixedRender *m)
@@ -729,11 +767,9 @@ fill_mixed_render(const RenderParams &p, double *data, double *info, double t_in
 	m->n_sub = n_sub;
 	for(int i = 0; i < GRAY_MAX_FREQ; ++i)
 		m->nu_hz[i] = p.nu[i];
-	m->m_adm = p.m_adm;
-	m->flow_te = p.flow_te;
-	m->flow_b = p.flow_b;
-	m->th = p.th;
 	m->thermal = p.flow == GRAY_FLOW_THERMAL;
+	if(m->thermal)
+		thermal_fast(p, &m->tf);
 }
 
 size_t

@@ -9,6 +9,25 @@
 
 #include "gray_internal.h"
 
+/* The thermal emissivities of rt.cl:80-170 with everything that depends
+ * only on the render's temperature, field and mass folded into per-render
+ * constants (FP64, on the host), so that per frequency and RHS only the
+ * frequency-dependent part is evaluated. */
+struct ThermalFast {
+	double kf2;       /* B_Planck: f2 = h nu / (m_e c^2 te) = nu kf2          */
+	double kB;        /* B = kB nu^3 / (e^f2 - 1), kB = 2 h / c^2              */
+	double kB2;       /* f2 <= 1e-5: B = kB2 nu^2 / (1 + f2/2 + f2^2/6)        */
+	double ky;        /* Gaunt y = nu ky                                      */
+	double xg, sxg;   /* Gaunt x (te only) and sqrt(x)                        */
+	double g1, g2, g3, g4, g5;
+	double kff;       /* L_ff = kff ne^2 G / (sqrt(te) e^y + EPS)              */
+	double sqte;      /* sqrt(te)                                             */
+	double knus;      /* nu_s = knus sin(theta)                               */
+	double ksyn;      /* L_syn = ksyn xx^2 e^-cbrt(x) ne nu_s                  */
+	double b;         /* field magnitude                                      */
+	int    syn;       /* te > T_MIN and b != 0 (else L_syn is exactly 0)      */
+};
+
 struct MixedRender {
 	float  a, aa, rp, risco, eps_stop;
 	float  cdt_scale;          /* 0.01: the step fraction of phys.cl:60-61     */
@@ -23,10 +42,9 @@ struct MixedRender {
 	long long n_rays;
 	double t_init, dt_dump;    /* dump i covers [t_init + i dt, t_init + (i+1) dt] */
 	long long n_sub;
-	/* thermal flow of numerical renders (FP64 transfer) */
+	/* thermal flow of numerical renders */
 	double nu_hz[GRAY_MAX_FREQ];
-	double m_adm, flow_te, flow_b;
-	ThermalConsts th;
+	ThermalFast tf;
 	int    thermal;
 };
 

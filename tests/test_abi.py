@@ -52,3 +52,23 @@ def test_desc_defaults_follow_reference_opts():
     assert (d.n_width, d.n_height) == (512, 512)
     assert (d.t_init, d.dt_dump, d.n_dump, d.n_sub) == (0.0, -32.0, 64, 1024)
     assert d.n_freq == 0 and d.flow == api.FLOW_NONE
+
+
+def test_bench_h2d_bytes_match_the_render_table(tmp_path):
+    """bench.py's host-to-device bytes per render are sizeof(MixedRender)."""
+    import shutil
+    import subprocess
+    import sys
+    cxx, inc = shutil.which("g++"), "/usr/local/cuda/include"
+    if not cxx or not os.path.isdir(inc):
+        import pytest
+        pytest.skip("no host compiler or CUDA headers")
+    src = tmp_path / "sz.cpp"
+    src.write_text('#include "%s"\n#include <cstdio>\nint main(){printf("%%zu", sizeof(MixedRender));}\n'
+                   % os.path.join(ROOT, "gray_b200", "csrc", "mixed_table.h"))
+    exe = tmp_path / "sz"
+    subprocess.run([cxx, "-I", inc, str(src), "-o", str(exe)], check=True)
+    size = int(subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout)
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.H2D_BYTES_PER_RENDER == size
