@@ -507,7 +507,7 @@ typedef void (*rhs_fn)(const void *ctx, const double *s, double *ds);
 static void
 rk4(rhs_fn fn, const void *ctx, int nd, double *s, double dt)
 {
-	double k1[NDMAX], k2[NDMAX], k3[NDMAX], k4[NDMAX], t[NDMAX];
+	double k1[NDMAX], k2[NDMAX], k3[NDMAX], k4[NDMAX], t[NDMAX] = {0.0};
 	double hdt = 0.5 * dt;
 	int i;
 	fn(ctx, s, k1);
