@@ -51,9 +51,11 @@ WORKLOADS = {"torus_rt_1024": configs.TORUS_RT_1024,
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 METRIC = "ray-steps/s"
 
-# DRAM bytes per launch of the dominant kernel from the committed ncu
-# capture (profiles/mixed_kernel_torus_rt.md), scaled to a full render.
-TRAFFIC = {}
+# DRAM bytes (read + write) of one full-size launch of the dominant kernel,
+# from one-pass ncu captures (profiles/mixed_kernel_torus_rt.md,
+# profiles/dyst_mixed_kernel_numerical_128.md).
+TRAFFIC = {"torus_rt_1024": 145832704 + 116188928,
+           "numerical_128": 504967168 + 19106048}
 # Host-to-device bytes of one render through the C ABI: the render's table
 # entry (sizeof(MixedRender) in gray_b200/csrc/mixed_table.h); the camera
 # initial conditions are generated on the device.
@@ -292,7 +294,7 @@ def ours_arm(args, cfg, rank, local_rank, world, dist):
     achieved = steps_per_render * flop_step / (ker / args.steps) / 1e12
     roofline = {"bound": "fp32", "achieved": achieved, "peak": peak32 / 1e12,
                 "unit": "TFLOP/s", "frac": achieved * 1e12 / peak32,
-                "traffic": TRAFFIC.get(args.workload),
+                "traffic": None if args.side else TRAFFIC.get(args.workload),
                 "peak_source": "FMA-loop microbenchmark in this run (best of scalar and f32x2 FFMA)",
                 "flop_per_ray_step": flop_step,
                 "kernel": "mixed_kernel<%d>" % nf}
@@ -552,7 +554,7 @@ def numerical_arm(args, cfg, rank, local_rank, world, dist):
         hbm = json.load(f)["hbm_gbs"]
     achieved = gsteps * GATHER_BYTES_PER_STEP / (ker / args.steps) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": None,
+                "frac": achieved / hbm, "traffic": None if args.side else TRAFFIC.get(args.workload),
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
                 "bytes_per_gather_step": GATHER_BYTES_PER_STEP,
                 "note": "algorithmic gather bytes; most hit L1/L2, so frac > 1 is cache reuse",
