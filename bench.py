@@ -101,7 +101,7 @@ def cpu_rate(cfg, seconds, max_batches=10 ** 6):
     batch = max(threads * 2, 16)
     stride = 7919  # prime stride: rays from every part of the image
     done_steps, done_rays, t_used, k = 0, 0, 0.0, 0
-    while t_used < seconds and k < max_batches:
+    while (k == 0 or t_used < seconds) and k < max_batches:  # at least one batch
         rays = (np.arange(k * batch, (k + 1) * batch, dtype=np.int64) * stride) % n_rays
         t0 = time.perf_counter()
         _, _, steps = O.trace(cfg, rays, nthreads=threads)

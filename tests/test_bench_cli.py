@@ -1,0 +1,35 @@
+"""bench.py's reference arm (the oracle port on the host cores) runs without
+a GPU: check its JSON line on a short run, and that ranks other than 0 of a
+multi-rank launch exit quietly."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def run(args, env=None):
+    e = dict(os.environ)
+    e.update(env or {})
+    return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py")] + args,
+                          capture_output=True, text=True, cwd=ROOT, env=e, timeout=600)
+
+
+def test_reference_arm_line():
+    p = run(["--impl", "reference", "--steps", "1", "--warmup", "3", "--cpu-seconds", "0.2"])
+    assert p.returncode == 0, p.stderr[-2000:]
+    line = json.loads(p.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["metric"] == "ray-steps/s"
+    assert line["value"] > 0 and line["higher_is_better"] is True
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"] == {"value": line["value"], "unit": "ray-steps/s",
+                           "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert line["config"]["workload"] == "torus_rt_1024"
+
+
+def test_reference_arm_other_ranks_exit_quietly():
+    p = run(["--impl", "reference", "--steps", "1", "--warmup", "3", "--gpus", "2"],
+            env={"RANK": "1", "LOCAL_RANK": "1", "WORLD_SIZE": "2"})
+    assert p.returncode == 0, p.stderr[-2000:]
+    assert p.stdout.strip() == ""
