@@ -79,7 +79,7 @@ def parse():
                     help="launch shape of the persistent kernel (measure = autotune)")
     ap.add_argument("--fp64-renders", type=int, default=16,
                     help="survey_256: renders run one at a time in FP64 for the comparison")
-    ap.add_argument("--rates", default="1,2,3,4,6,8,12",
+    ap.add_argument("--rates", default="0.5,1,2,3,4,6,8,12",
                     help="serve_mix: arrival rates (requests/s) swept in order")
     ap.add_argument("--requests", type=int, default=32, help="serve_mix: requests per rate")
     ap.add_argument("--partition", default="replicate", choices=["replicate", "split"],
@@ -626,8 +626,11 @@ def numerical_arm(args, cfg, rank, local_rank, world, dist):
 def serve_arm(args, rank, local_rank, world, dist):
     """serve_mix: seeded Poisson arrivals of analytic (70%) and numerical
     (30%) render requests into the continuous-batching server, with a
-    device-resident 256^3 grid and a 120 GB admission budget; the arrival
-    rate is swept upward until p99 latency exceeds 4 x p50."""
+    device-resident 256^3 grid and a 120 GB admission budget.  The arrival
+    rate is swept upward over the whole list; the sustained rate is the
+    highest one whose p99 latency stays within 4x the p50 of the lowest
+    rate (the unloaded latency), and `value` is the highest throughput of
+    the sweep (the server's capacity on this mix)."""
     import time
     import torch
     from gray_b200 import api
@@ -643,7 +646,7 @@ def serve_arm(args, rank, local_rank, world, dist):
     rng = np.random.Generator(np.random.PCG64(configs.SERVE_SEED + 1))
     budget = int(120e9)
     ctx.serve_start(hbm_budget=budget, max_inflight=256, dumps_per_iter=args.dumps_per_iter)
-    sweep, sustained, k0 = [], None, 0
+    sweep, sustained, within, k0 = [], None, True, 0
     sample = {}  # class -> (cfg, served state) for the FP64 comparison
     try:
         # warm-up: one request of each kind
@@ -694,9 +697,9 @@ def serve_arm(args, rank, local_rank, world, dist):
                    "p50_by_class": {k: float(np.percentile(lat[np.array(kinds) == k], 50))
                                      for k in set(kinds)}}
             sweep.append(row)
-            if p99 > 4 * p50:
-                break
-            sustained = row
+            within &= p99 <= 4 * sweep[0]["p50_s"]
+            if within:
+                sustained = row
         stats, _ = ctx.serve_stats()
     finally:
         ctx.serve_stop()
@@ -726,9 +729,10 @@ def serve_arm(args, rank, local_rank, world, dist):
     if rank != 0:
         return
     best = sustained or sweep[0]
+    peak = max(sweep, key=lambda r: r["throughput"])
     line = {
-        "metric": METRIC, "value": best["throughput"], "unit": "ray-steps/s", "n_gpus": world,
-        "steps": len(sweep), "warmup": 1, "ms_per_step": 1e3 * best["wall_s"],
+        "metric": METRIC, "value": peak["throughput"], "unit": "ray-steps/s", "n_gpus": world,
+        "steps": len(sweep), "warmup": 1, "ms_per_step": 1e3 * peak["wall_s"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64-islands", "data": "synthetic",
         "config": {"workload": "serve_mix", "requests_per_rate": args.requests,
@@ -737,11 +741,14 @@ def serve_arm(args, rank, local_rank, world, dist):
                    "hbm_budget_bytes": budget, "dumps_per_iter": args.dumps_per_iter,
                    "mix": "70% analytic torus 64..1024^2, 30% numerical 64..512^2"},
         "latency": {"p50_s": best["p50_s"], "p99_s": best["p99_s"],
-                    "sustained_rate_per_s": best["rate_per_s"]},
+                    "sustained_rate_per_s": best["rate_per_s"],
+                    "rule": "highest rate with p99 <= 4 x the p50 of the lowest rate",
+                    "unloaded_p50_s": sweep[0]["p50_s"],
+                    "peak_throughput_rate_per_s": peak["rate_per_s"]},
         "sweep": sweep, "error_vs_fp64": errs,
         "serve_stats": {"iterations": stats.iterations, "busy_s": stats.busy_s,
                         "completed": stats.completed},
-        "e2e": {"value": best["throughput"], "unit": "ray-steps/s",
+        "e2e": {"value": peak["throughput"], "unit": "ray-steps/s",
                 "note": "request submit to result in host memory, host clock"},
     }
     print(json.dumps(line), flush=True)
