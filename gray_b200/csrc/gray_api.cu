@@ -438,9 +438,20 @@ gray_render_create(gray_ctx *c, const gray_render_desc *d, int *id)
 	r->d_queue = (unsigned int *)((char *)base + data_b + info_b + 128);
 	r->d_prefix = (unsigned long long *)((char *)base + data_b + info_b + 192);
 	r->d_table = (MixedRender *)((char *)base + data_b + info_b + 256);
-	CK(cudaMemsetAsync((char *)base + data_b + info_b, 0, 256, c->stream));
+	cudaError_t e = cudaMemsetAsync((char *)base + data_b + info_b, 0, 256, c->stream);
+	if(e != cudaSuccess) {
+		dfree(c, base, r->bytes);
+		delete r;
+		return from_cuda(e);
+	}
+	try {
+		c->renders[c->next_id] = r;
+	} catch(const std::bad_alloc &) {
+		dfree(c, base, r->bytes);
+		delete r;
+		return GRAY_ENOMEM;
+	}
 	*id = c->next_id++;
-	c->renders[*id] = r;
 	return GRAY_OK;
 }
 
@@ -828,8 +839,15 @@ ensure_grid(gray_ctx *c, const gray_grid_desc *gd)
 			double A = (cbrt(asinh(hi)) - B) / (double)(n[a] - 1);
 			gp.A[a] = A;
 			gp.B[a] = B;
-			std::vector<double> nd(n[a] + 1);
-			std::vector<float> nf(n[a] + 1);
+			std::vector<double> nd;
+			std::vector<float> nf;
+			try {
+				nd.resize(n[a] + 1);
+				nf.resize(n[a] + 1);
+			} catch(const std::bad_alloc &) {
+				free_grid(c);
+				return GRAY_ENOMEM;
+			}
 			for(int i = 0; i <= n[a]; ++i) {
 				double f = fma(A, (double)i, B);
 				nd[i] = sinh((f * f) * f);
@@ -1058,8 +1076,15 @@ gray_batch_create(gray_ctx *c, const int *ids, int n, int *batch_id)
 	Batch *b = new(std::nothrow) Batch;
 	if(!b)
 		return GRAY_ENOMEM;
-	b->host_table.resize(n);
-	std::vector<unsigned long long> prefix(n);
+	std::vector<unsigned long long> prefix;
+	try { /* no exception may cross the C ABI */
+		b->host_table.resize(n);
+		b->ids.reserve(n);
+		prefix.resize(n);
+	} catch(const std::bad_alloc &) {
+		delete b;
+		return GRAY_ENOMEM;
+	}
 	for(int i = 0; i < n; ++i) {
 		Render *r = find(c, ids[i]);
 		if(!r) {
@@ -1118,8 +1143,14 @@ gray_batch_create(gray_ctx *c, const int *ids, int n, int *batch_id)
 		delete b;
 		return from_cuda(e);
 	}
+	try {
+		c->batches[c->next_batch] = b;
+	} catch(const std::bad_alloc &) {
+		dfree(c, b->block, b->bytes);
+		delete b;
+		return GRAY_ENOMEM;
+	}
 	*batch_id = c->next_batch++;
-	c->batches[*batch_id] = b;
 	return GRAY_OK;
 }
 
@@ -1292,7 +1323,12 @@ gray_plan(gray_ctx *c, int id, int flags, gray_launch_plan *best)
 		return gray_get_plan(c, best);
 	}
 	/* trial table: the first two dump intervals of every render */
-	std::vector<MixedRender> trial = b->host_table;
+	std::vector<MixedRender> trial;
+	try {
+		trial = b->host_table;
+	} catch(const std::bad_alloc &) {
+		return GRAY_ENOMEM;
+	}
 	for(auto &m : trial)
 		m.dump_end = m.dump_begin + (m.dump_end - m.dump_begin > 2 ? 2 : m.dump_end - m.dump_begin);
 	CK(cudaMemcpyAsync(b->d_table, trial.data(), trial.size() * sizeof(MixedRender),

@@ -167,7 +167,7 @@ load_rc(RC<V, NF> &rc, int k, const MixedRender &c)
 
 template <typename V>
 struct Aux {
-	V r, ir, f, lx, ly, lz, flu, iss;
+	V r, ir, f, lx, ly, lz, flu, iss, R2;
 };
 
 /* KS.cl:263-378 in FP32: the Chan et al. grouping, with the five divides
@@ -185,15 +185,15 @@ ks_rhs(const RC<V, NF> &c, const V *s, V *ds, Aux<V> &aux)
 	V lx, dx_lx, dy_lx, dz_lx;
 	V ly, dx_ly, dy_ly, dz_ly;
 	V lz, dx_lz, dy_lz, dz_lz;
-	V dx_r, dy_r, dz_r, r, ir, iss, tmp;
+	V dx_r, dy_r, dz_r, r, ir, iss, tmp, R2;
 	{
 		V zz  = z * z;
 		V azz = aa * zz;
-		V kk  = half * (fmav(x, x, fmav(y, y, zz)) - aa);
+		R2       = fmav(x, x, y * y); /* also the torus's cylindrical radius */
+		V kk  = half * ((R2 + zz) - aa);
 		V d2  = fmav(kk, kk, azz);
 		V idd = rsqv(d2);
-		V dd  = d2 * idd;
-		V rr  = dd + kk;
+		V rr  = fmav(d2, idd, kk);    /* sqrt(d2) + kk */
 		ir  = rsqv(rr);
 		r   = rr * ir;
 		V ss = rr + aa;
@@ -272,7 +272,7 @@ ks_rhs(const RC<V, NF> &c, const V *s, V *ds, Aux<V> &aux)
 	ds[6] = fmav(ly, tmp, hDyu - uD2);
 	ds[7] = fmav(lz, tmp, hDzu - uD3);
 
-	aux.r = r; aux.ir = ir; aux.f = f; aux.lx = lx; aux.ly = ly; aux.lz = lz;
+	aux.r = r; aux.ir = ir; aux.f = f; aux.lx = lx; aux.ly = ly; aux.lz = lz; aux.R2 = R2;
 	aux.flu = flu; aux.iss = iss;
 	(void)one;
 }
@@ -290,7 +290,7 @@ torus_rt(const RC<V, NF> &c, const V *s, const Aux<V> &x, V *ds)
 	V kt  = x.flu - s[4];
 	V kx  = fmav(x.flu, x.lx, s[5]);
 	V ky  = fmav(x.flu, x.ly, s[6]);
-	V R2  = fmav(q1, q1, q2 * q2);
+	const V R2 = x.R2;
 	V irs = rsqv(x.r);                 /* r^-1/2 */
 	V sr  = x.r * irs;                 /* r^1/2  */
 	V Om  = rcpv(fmav(x.r, sr, c.a));

@@ -201,7 +201,12 @@ gray_run_series(gray_ctx *c, int id, const gray_grid_desc *gd,
 	if(c->server)
 		return GRAY_ESTATE; /* the server's renders read the grid */
 	const gray_render_desc &d = r->desc;
-	std::vector<int64_t> pairs(d.n_dump ? d.n_dump : 1);
+	std::vector<int64_t> pairs;
+	try { /* no exception may cross the C ABI */
+		pairs.resize(d.n_dump ? d.n_dump : 1);
+	} catch(const std::exception &) {
+		return GRAY_ENOMEM;
+	}
 	int64_t first;
 	bool frozen;
 	int st = schedule(src->times, src->n_times, d.t_init, d.dt_dump, d.n_dump, fast_light,

@@ -255,6 +255,12 @@ loop(Server *S)
 	cudaSetDevice(S->c->device);
 	for(;;) {
 		std::vector<Request *> fresh;
+		try { /* admission below never grows it past this */
+			fresh.reserve((size_t)S->cfg.max_inflight);
+		} catch(const std::bad_alloc &) {
+			std::this_thread::sleep_for(std::chrono::milliseconds(20));
+			continue;
+		}
 		{
 			std::unique_lock<std::mutex> lk(S->mu);
 			if(S->inflight.empty())
@@ -284,7 +290,12 @@ loop(Server *S)
 				++slots;
 			}
 		}
-		int st = iterate(S, fresh);
+		int st;
+		try { /* a failed host allocation ends serving like a device error */
+			st = iterate(S, fresh);
+		} catch(const std::bad_alloc &) {
+			st = GRAY_ENOMEM;
+		}
 		if(st) {
 			/* device failure: fail everything in flight and stop serving */
 			std::lock_guard<std::mutex> lk(S->mu);
@@ -449,17 +460,24 @@ gray_serve_submit(gray_ctx *c, const gray_render_desc *d, uint64_t *id)
 			delete r;
 			return GRAY_ESTATE;
 		}
-		r->id = S->next_id++;
+		r->id = S->next_id;
 		r->t_submit = now_s();
+		try { /* no exception may cross the C ABI */
+			S->reqs[r->id] = r;
+			if(r->bytes <= S->budget)
+				S->pending.push_back(r);
+		} catch(const std::bad_alloc &) {
+			S->reqs.erase(r->id);
+			delete r;
+			return GRAY_ENOMEM;
+		}
+		++S->next_id;
 		if(r->bytes > S->budget) { /* can never be admitted */
 			r->state = GRAY_REQ_FAILED;
 			r->status = GRAY_EBUDGET;
 			r->t_done = r->t_submit;
 			S->stats.failed++;
-		} else {
-			S->pending.push_back(r);
 		}
-		S->reqs[r->id] = r;
 		*id = r->id;
 	}
 	S->cv.notify_all();
