@@ -1,0 +1,91 @@
+"""Edge cases of the analytic path against the CPU oracle: retrograde and
+near-extremal spin, pole-on and edge-on cameras, non-square and one-ray
+images, forward tracing, the r_+ stop rule, zero dump intervals, and the
+transfer at one and eight frequencies.  FP64 within the 1e-10 parity bar
+(the geodesic is bit-identical); mixed images within 1e-4 of FP64 and end
+positions within 1e-3 (L2 over the rays that stay away from the horizon)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from gray_b200 import api
+
+BASE = dict(a_spin=0.9, r_obs=200.0, i_obs=60.0, j_obs=0.0, w_img=30.0, h_img=30.0,
+            n_width=6, n_height=5, t_init=0.0, dt_dump=-40.0, n_dump=10, n_sub=200)
+
+CASES = {
+    "retrograde": dict(a_spin=-0.9),
+    "near_extremal": dict(a_spin=0.999),
+    "schwarzschild": dict(a_spin=0.0),
+    "pole_on": dict(i_obs=0.0),
+    "edge_on": dict(i_obs=90.0, j_obs=45.0),
+    "non_square": dict(n_width=7, n_height=3, w_img=40.0, h_img=12.0),
+    "one_ray": dict(n_width=1, n_height=1),
+    "forward": dict(dt_dump=25.0, n_dump=4),
+    "rplus_stop": dict(term=api.TERM_RPLUS),
+    "no_dumps": dict(n_dump=0),
+    "one_frequency": dict(nu=(1.0,), torus_kappa=125.8988),
+    "eight_frequencies": dict(nu=tuple(2.0 ** (i - 3) for i in range(8)), torus_kappa=125.8988),
+}
+
+
+def gpu(ctx, cfg, prec):
+    r = ctx.render(dict(cfg, precision=prec))
+    try:
+        r.run()
+        d, info = r.state(api.LAYOUT_AOS)
+        return d, info, r.steps()
+    finally:
+        r.close()
+
+
+def test_cases_are_valid_for_the_oracle():
+    for name, kw in CASES.items():
+        cfg = dict(BASE, **kw)
+        n = cfg["n_width"] * cfg["n_height"]
+        out, info, _ = O.trace(cfg, np.arange(min(n, 3)))
+        assert out.shape[1] == 8 + 2 * len(cfg.get("nu", ())), name
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fp64_edge_case_matches_oracle(ctx, name):
+    cfg = dict(BASE, **CASES[name])
+    n = cfg["n_width"] * cfg["n_height"]
+    g, ginfo, gsteps = gpu(ctx, cfg, api.PREC_FP64)
+    o, oinfo, osteps = O.trace(cfg, np.arange(n))
+    assert gsteps == osteps.sum()
+    fin = np.all(np.isfinite(o), axis=1)
+    assert np.array_equal(fin, np.all(np.isfinite(g), axis=1))
+    assert np.array_equal(g[fin, :8], o[fin, :8]), name  # geodesic: bit for bit
+    if o.shape[1] > 8:
+        scale = np.maximum(np.abs(o[fin, 8:]).max(axis=0), 1e-300)
+        assert np.max(np.abs(g[fin, 8:] - o[fin, 8:]) / scale) <= 1e-10
+    assert np.allclose(ginfo[fin], oinfo[fin], rtol=0, atol=1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_mixed_edge_case_close_to_fp64(ctx, name):
+    cfg = dict(BASE, **CASES[name])
+    g64, _, s64 = gpu(ctx, cfg, api.PREC_FP64)
+    gmx, _, smx = gpu(ctx, cfg, api.PREC_MIXED)
+    fin = np.all(np.isfinite(g64), axis=1) & np.all(np.isfinite(gmx), axis=1)
+    rp = 1.0 + np.sqrt(1.0 - cfg["a_spin"] ** 2)
+    r64 = np.linalg.norm(g64[:, 1:4], axis=1)
+    esc = fin & (r64 > 3.0 * rp)  # rays away from the horizon
+    if cfg["n_dump"] == 0:
+        # icond only: the FP64 camera state through one (hi, lo) FP32 round trip
+        assert np.allclose(gmx, g64, rtol=1e-13, atol=1e-13)
+        return
+    if esc.any():
+        # end positions: rays that graze the photon orbit amplify rounding, so
+        # the bar is on the L2 over all escaping rays; the image bar is 1e-4
+        pos = np.linalg.norm(gmx[esc, 1:4] - g64[esc, 1:4]) / np.linalg.norm(g64[esc, 1:4])
+        assert pos <= 1e-3, (name, pos)
+        for i in range(len(cfg.get("nu", ()))):
+            ref = g64[esc, 8 + i]
+            if np.abs(ref).max() > 0:
+                e = np.linalg.norm(gmx[esc, 8 + i] - ref) / np.linalg.norm(ref)
+                assert e <= 1e-4, (name, i, e)
+    assert abs(smx - s64) <= 0.01 * s64 + 64
