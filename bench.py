@@ -85,7 +85,7 @@ def parse():
     ap.add_argument("--partition", default="replicate", choices=["replicate", "split"],
                     help="survey_256 on N GPUs: every rank renders the survey (weak) or "
                          "the renders are split across ranks (strong)")
-    ap.add_argument("--dumps-per-iter", type=int, default=4,
+    ap.add_argument("--dumps-per-iter", type=int, default=16,
                     help="serve_mix: dump intervals each server iteration advances")
     return ap.parse_args()
 
