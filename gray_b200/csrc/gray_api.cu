@@ -118,6 +118,9 @@ check_desc(const gray_render_desc *d)
 			return GRAY_EINVAL;
 	if(!std::isfinite(d->dt_dump) || !std::isfinite(d->t_init))
 		return GRAY_EINVAL;
+	/* driver.cl:93 divides by the interval: a zero one has no step count */
+	if(d->n_dump > 0 && d->dt_dump == 0.0)
+		return GRAY_EINVAL;
 	return GRAY_OK;
 }
 
@@ -561,9 +564,11 @@ gray_evolve(gray_ctx *c, int id, double t, double target, uint64_t n_sub, double
 	int st = timed_begin(c);
 	if(st)
 		return st;
-	st = evolve_interval(c, r, t, target, n_sub);
-	if(st)
-		return st;
+	if(target != t) { /* an empty interval leaves the state as it is */
+		st = evolve_interval(c, r, t, target, n_sub);
+		if(st)
+			return st;
+	}
 	return timed_end(c, ns);
 }
 

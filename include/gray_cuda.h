@@ -141,8 +141,9 @@ int gray_icond(gray_ctx *ctx, int render_id);
 
 /* Replaces evolve() (sim-org/evolve.c:28-67 -> driver.cl:69-108 evolve_drv):
  * integrates every ray over one dump interval of affine length target - t
- * with n_sub substeps.  If ns is non-NULL the call waits and stores the
- * kernel time in ns (what ocl->exec returns); otherwise it only enqueues. */
+ * with n_sub substeps (target == t leaves the state unchanged).  If ns is
+ * non-NULL the call waits and stores the kernel time in ns (what ocl->exec
+ * returns); otherwise it only enqueues. */
 int gray_evolve(gray_ctx *ctx, int render_id, double t, double target,
                 uint64_t n_sub, double *ns);
 

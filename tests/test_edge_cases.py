@@ -89,3 +89,23 @@ def test_mixed_edge_case_close_to_fp64(ctx, name):
                 e = np.linalg.norm(gmx[esc, 8 + i] - ref) / np.linalg.norm(ref)
                 assert e <= 1e-4, (name, i, e)
     assert abs(smx - s64) <= 0.01 * s64 + 64
+
+
+@pytest.mark.gpu
+def test_zero_length_intervals(ctx):
+    """A zero dump interval has no step count (driver.cl:93 divides by it):
+    rejected when there are dumps to take, and an evolve from t to t leaves
+    the state as it is."""
+    with pytest.raises(api.GrayError) as e:
+        ctx.render(dict(BASE, dt_dump=0.0))
+    assert e.value.status == api.EINVAL
+    for prec in (api.PREC_FP64, api.PREC_MIXED):
+        r = ctx.render(dict(BASE, dt_dump=0.0, n_dump=0, precision=prec))
+        try:
+            r.icond()
+            before, _ = r.state()
+            r.evolve(5.0, 5.0)
+            after, _ = r.state()
+            assert np.array_equal(before, after)
+        finally:
+            r.close()
