@@ -391,6 +391,56 @@ gray_write_raw(const char *path, const double *data, const double *info,
 	return (fclose(f) == 0 && ok) ? GRAY_OK : GRAY_EINVAL;
 }
 
+int
+gray_read_raw(const char *path, double *data, double *info, size_t n_data, size_t w, size_t h)
+{
+	size_t hdr[4];
+	const size_t n_rays = w * h;
+	if(!path || !data || !info)
+		return GRAY_EINVAL;
+	FILE *f = fopen(path, "rb");
+	if(!f)
+		return GRAY_ENOTFOUND;
+	int st = GRAY_OK;
+	if(fread(hdr, sizeof(size_t), 4, f) != 4 || hdr[0] != sizeof(double) ||
+	   hdr[1] != n_data || hdr[2] != w || hdr[3] != h)
+		st = GRAY_ESIZE;
+	else if(fread(data, sizeof(double) * n_data, n_rays, f) != n_rays ||
+	        fread(info, sizeof(double), n_rays, f) != n_rays)
+		st = GRAY_ESIZE;
+	fclose(f);
+	return st;
+}
+
+/* Resume at dump i_init from the dump file a previous run wrote there
+ * (the checkpoint the reference's dumps are but cannot load, io.c:37).
+ * GRAY_ENOTFOUND when there is no such file: the run then starts from the
+ * camera as the reference does. */
+static int
+resume(struct gray_job *j, size_t i)
+{
+	if(!j->outfile[0] || i == 0)
+		return GRAY_ENOTFOUND;
+	gray_render_desc d;
+	gray_job_desc(&j->super, &d);
+	const size_t n_rays = d.n_width * d.n_height;
+	const size_t n_data = 8 + 2 * (size_t)d.n_freq;
+	double *data = malloc(sizeof(double) * n_rays * n_data);
+	double *info = malloc(sizeof(double) * n_rays);
+	int st = (data && info) ? GRAY_OK : GRAY_ENOMEM;
+	if(!st) {
+		char name[512];
+		snprintf(name, sizeof(name), j->outfile, (int)i);
+		st = gray_read_raw(name, data, info, n_data, d.n_width, d.n_height);
+	}
+	if(!st)
+		st = gray_write_state(j->ctx, j->render, data, sizeof(double) * n_rays * n_data,
+		                      GRAY_LAYOUT_AOS);
+	free(data);
+	free(info);
+	return st;
+}
+
 /* sim-org/io.c:39-72 dump(): state in AoS with its info diagnostic */
 static int
 dump(struct gray_job *j, size_t i)
@@ -444,13 +494,19 @@ exec(gray_lux_job *ego)
 	if(!j->ctx)
 		return GRAY_ESTATE;
 	const double n_rays = (double)j->n_width * (double)j->n_height;
-	int st = gray_icond(j->ctx, j->render);
-	if(st)
-		return st;
-	printf("%zu:  initialize at %4.1f", i, j->t_init);
-	if((st = dump(j, i)))
-		return st;
-	printf(": DONE\n");
+	int st = resume(j, i);
+	if(st == GRAY_OK) {
+		printf("%zu:  resumed from its dump\n", i);
+	} else if(st == GRAY_ENOTFOUND) {
+		if((st = gray_icond(j->ctx, j->render)))
+			return st;
+		printf("%zu:  initialize at %4.1f", i, j->t_init);
+		if((st = dump(j, i)))
+			return st;
+		printf(": DONE\n");
+	} else {
+		return st; /* a dump is there but does not fit this run */
+	}
 	while(i < j->n_dump) {
 		double ns;
 		double t      = j->t_init + (double)i * j->dt_dump;

@@ -56,6 +56,13 @@ int gray_job_stats(const gray_lux_job *ego, uint64_t *ray_steps, double *kernel_
 int gray_write_raw(const char *path, const double *data, const double *info,
                    size_t n_data, size_t w, size_t h);
 
+/* Reads a dump gray_write_raw wrote, after checking that its header is
+ * {8, n_data, w, h}: the load path sim-org/io.c:37 leaves as a TODO.
+ * GRAY_ENOTFOUND when the file does not open, GRAY_ESIZE on a header or
+ * length mismatch. */
+int gray_read_raw(const char *path, double *data, double *info, size_t n_data, size_t w,
+                  size_t h);
+
 #ifdef __cplusplus
 }
 #endif
