@@ -289,17 +289,21 @@ def fisheye_nodes(lo, hi, n):
 
 
 def boosted_ks_grid(n, lo, hi, t, m=1.0, a=0.7, v=0.3, axis=1, rho=True):
-    """Sample the boosted KS fields on an n^3 fisheye grid (slow, for small n)."""
-    xs = fisheye_nodes(lo, hi, n)
-    out = np.zeros((n, n, n, 51), dtype=np.float64)
+    """Sample the boosted KS fields on a fisheye grid (slow, for small n).
+    n, lo, hi are numbers (a cube) or (x, y, z) triples."""
+    n3 = (n,) * 3 if np.isscalar(n) else tuple(n)
+    lo3 = (lo,) * 3 if np.isscalar(lo) else tuple(lo)
+    hi3 = (hi,) * 3 if np.isscalar(hi) else tuple(hi)
+    ax = [fisheye_nodes(lo3[c], hi3[c], n3[c]) for c in range(3)]
+    out = np.zeros((n3[2], n3[1], n3[0], 51), dtype=np.float64)
     L = lib()
     q = np.zeros(4)
     buf = np.zeros(50)
     # the origin node (odd n) gives rho = 1/0 = inf, as tools/generate_data.py does
     with np.errstate(divide="ignore", over="ignore", invalid="ignore"):
-        for k, z in enumerate(xs):
-            for j, y in enumerate(xs):
-                for i, x in enumerate(xs):
+        for k, z in enumerate(ax[2]):
+            for j, y in enumerate(ax[1]):
+                for i, x in enumerate(ax[0]):
                     q[:] = (t, x, y, z)
                     L.orc_boosted_ks(m, a, v, axis, _p(q), _p(buf))
                     out[k, j, i, :50] = buf
