@@ -737,7 +737,7 @@ def serve_arm(args, rank, local_rank, world, dist):
         "dtype": "f32+f64-islands", "data": "synthetic",
         "config": {"workload": "serve_mix", "requests_per_rate": args.requests,
                    "grid": "%d^3 FP32 boosted KS (a=0.7, v=0.3 along x), %.2f GB" %
-                           (n, n ** 3 * 52 * 4 / 1e9),
+                           (n, n ** 3 * 56 * 4 / 1e9),
                    "hbm_budget_bytes": budget, "dumps_per_iter": args.dumps_per_iter,
                    "mix": "70% analytic torus 64..1024^2, 30% numerical 64..512^2"},
         "latency": {"p50_s": best["p50_s"], "p99_s": best["p99_s"],

@@ -54,7 +54,7 @@ void gray_thermal_consts(ThermalConsts *t);
 
 /* Numerical spacetime on the device: two time levels, each interleaved
  * [z][y][x][GRAY_NSTRIDE] floats, plus per-axis fisheye node tables. */
-#define GRAY_NSTRIDE 52      /* 51 fields padded to a 16-byte multiple    */
+#define GRAY_NSTRIDE 56      /* 51 fields padded to a 32-byte multiple    */
 struct GridParams {
 	int    nx, ny, nz;
 	float  box[8];

@@ -6,8 +6,8 @@
  *
  * Grid layout: per time level float [nz][ny][nx][GRAY_NSTRIDE] with the
  * fields of one grid point contiguous (Gamma 0..39, g 40..49, rho 50, pad),
- * so the 8 corners of a cell are 8 rows of 208 bytes and the 40 Gamma of a
- * corner are 10 aligned float4 loads.  The fisheye node coordinates come
+ * so the 8 corners of a cell are 8 rows of 224 bytes and the 40 Gamma of a
+ * corner are 5 aligned 32-byte loads (sm_100 ld.global.v8.f32).  The fisheye node coordinates come
  * from a per-axis table (n + 1 entries) instead of sinh((A i + B)^3) per
  * field and call (interp.cl:99-121), and the cell search runs once per RHS
  * for all fields instead of once per field (102 times in the reference).
@@ -86,6 +86,23 @@ axis_uvw32(const GridParams &g, int a, float x, float Bf, float iAf)
 struct DystConst {
 	float B[3], iA[3];
 };
+
+/* eight consecutive floats from a 32-byte aligned address, through the
+ * read-only path */
+struct F8 {
+	float v[8];
+};
+
+__device__ __forceinline__ F8
+ldg8(const float *p)
+{
+	F8 r;
+	asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+	    : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]), "=f"(r.v[4]), "=f"(r.v[5]),
+	      "=f"(r.v[6]), "=f"(r.v[7])
+	    : "l"(p));
+	return r;
+}
 
 /* ------------------------------------------------ thermal transfer island */
 
@@ -263,24 +280,26 @@ dyst_rhs32(const GridParams &g, const DystConst &dc, const float *s, float *ds,
 			if(!(l ? use1 : use0))
 				continue;
 			float wl = g.single ? wc : wc * (l ? ft : 1.0f - ft);
-			const float4 *src = (const float4 *)(g.lvl[l] + row);
+			const float *src = g.lvl[l] + row;
 			float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
-			for(int k = 0; k < 10; ++k) {
-				float4 v = __ldg(src + k);
-				const float e[4] = {v.x, v.y, v.z, v.w};
+			for(int k = 0; k < 5; ++k) {
+				const F8 v = ldg8(src + 8 * k);
 #pragma unroll
-				for(int q = 0; q < 4; ++q) {
-					const int idx = 4 * k + q; /* Gamma^(idx/10)_(idx%10) */
-					s[idx / 10] = fmaf(e[q], p[idx % 10], s[idx / 10]);
+				for(int q = 0; q < 8; ++q) {
+					const int idx = 8 * k + q; /* Gamma^(idx/10)_(idx%10) */
+					s[idx / 10] = fmaf(v.v[q], p[idx % 10], s[idx / 10]);
 				}
 			}
 #pragma unroll
 			for(int m = 0; m < 4; ++m)
 				Gm[m] = fmaf(wl, s[m], Gm[m]);
 			if(RT) {
-				/* g_tt g_tx g_ty g_tz | g_xx g_xy g_xz g_yy | g_yz g_zz rho pad */
-				const float4 a = __ldg(src + 10), b = __ldg(src + 11), d = __ldg(src + 12);
+				/* g_tt g_tx g_ty g_tz g_xx g_xy g_xz g_yy | g_yz g_zz rho pad */
+				const F8 ab = ldg8(src + 40), de = ldg8(src + 48);
+				const float4 a = make_float4(ab.v[0], ab.v[1], ab.v[2], ab.v[3]);
+				const float4 b = make_float4(ab.v[4], ab.v[5], ab.v[6], ab.v[7]);
+				const float4 d = make_float4(de.v[0], de.v[1], de.v[2], de.v[3]);
 				const float gzz = g.bug_gzz ? d.x : d.y;
 				const float k0 = fmaf(a.w, u[3], fmaf(a.z, u[2], fmaf(a.y, u[1], a.x * u[0])));
 				const float k1 = fmaf(b.z, u[3], fmaf(b.y, u[2], fmaf(b.x, u[1], a.y * u[0])));

@@ -186,7 +186,8 @@ boosted_ks_kernel(const GridParams g, float *__restrict__ lvl, double m, double 
 			out[k++] = to_f32(gd[i][j]);
 	/* generate_data.py:124-128: rho = 1 / r */
 	out[50] = to_f32(1.0 / sqrt(q[1] * q[1] + q[2] * q[2] + q[3] * q[3]));
-	out[51] = 0.0f;
+	for(int pad = GRAY_NCOMP; pad < GRAY_NSTRIDE; ++pad)
+		out[pad] = 0.0f;
 }
 
 inline unsigned
