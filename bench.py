@@ -55,7 +55,7 @@ METRIC = "ray-steps/s"
 # from one-pass ncu captures (profiles/mixed_kernel_torus_rt.md,
 # profiles/dyst_mixed_kernel_numerical_128.md).
 TRAFFIC = {"torus_rt_1024": 145832704 + 116188928,
-           "numerical_128": 504967168 + 19106048}
+           "numerical_128": 500394240 + 17862656}
 # Host-to-device bytes of one render through the C ABI: the render's table
 # entry (sizeof(MixedRender) in gray_b200/csrc/mixed_table.h); the camera
 # initial conditions are generated on the device.
@@ -550,6 +550,27 @@ def numerical_arm(args, cfg, rank, local_rank, world, dist):
     ker = max_over_ranks(torch, dist, ker)
     value = world * steps * args.steps / tot
     mixed_state = rm.state(api.LAYOUT_SOA)[0]
+    # end to end through the C ABI: each step renders from the camera on the
+    # resident grid and reads the whole state back into pinned host memory
+    n_rays = cfg["n_width"] * cfg["n_height"]
+    host = torch.empty(8 * n_rays, dtype=torch.float64, pin_memory=True).numpy().reshape(8, n_rays)
+    hinfo = torch.empty(n_rays, dtype=torch.float64, pin_memory=True).numpy()
+    barrier(torch, dist)
+    e2e_t = 0.0
+    for _ in range(args.e2e_steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rm.run(wait=False)
+        rm.state(api.LAYOUT_SOA, out=host, info_out=hinfo)  # synchronous d2h
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_t += e0.elapsed_time(e1) * 1e-3
+    barrier(torch, dist)
+    e2e_t = max_over_ranks(torch, dist, e2e_t)
+    e2e = {"value": world * steps * args.e2e_steps / e2e_t, "unit": "ray-steps/s",
+           "h2d_bytes_per_step": H2D_BYTES_PER_RENDER,
+           "d2h_bytes_per_step": int(host.nbytes + hinfo.nbytes)}
     with open(MEASURED_PEAKS) as f:
         hbm = json.load(f)["hbm_gbs"]
     achieved = gsteps * GATHER_BYTES_PER_STEP / (ker / args.steps) / 1e9
@@ -596,13 +617,18 @@ def numerical_arm(args, cfg, rank, local_rank, world, dist):
         og = O.Grid(lv, [G["t1"], -G["box"], -G["box"], -G["box"], G["t2"], G["box"], G["box"],
                          G["box"]], physics=True)
         threads = os.cpu_count() or 1
-        rays = (np.arange(threads * 2, dtype=np.int64) * 7919) % (cfg["n_width"] * cfg["n_height"])
-        t0 = time.perf_counter()
-        _, _, st = O.dyst_trace(cfg, og, rays, nthreads=threads)
-        secs = time.perf_counter() - t0
-        cpu = {"value": float(st.sum()) / secs, "unit": "ray-steps/s", "cores": threads,
+        batch, k, secs, done, nr = threads * 2, 0, 0.0, 0, 0
+        while k == 0 or secs < args.cpu_seconds:
+            rays = (np.arange(k * batch, (k + 1) * batch, dtype=np.int64) * 7919) % n_rays
+            t0 = time.perf_counter()
+            _, _, st = O.dyst_trace(cfg, og, rays, nthreads=threads)
+            secs += time.perf_counter() - t0
+            done += int(st.sum())
+            nr += batch
+            k += 1
+        cpu = {"value": done / secs, "unit": "ray-steps/s", "cores": threads,
                "kind": "port", "sample": "%d rays of numerical_128 (stride 7919), %.1f s"
-                                         % (len(rays), secs)}
+                                         % (nr, secs)}
     rm.close()
     ctx.close()
     if rank != 0:
@@ -617,7 +643,7 @@ def numerical_arm(args, cfg, rank, local_rank, world, dist):
                    "ray_steps_per_render": steps, "gather_steps_per_render": gsteps,
                    "mode": "physics (flat outside the box, time factor clamped)",
                    "l2": "flushed (256 MiB write) between steps"},
-        "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": 2 * args.steps,
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 2 * args.steps,
         "clocks": clocks, "fp64": fp64,
     }
     print(json.dumps(line), flush=True)
