@@ -57,35 +57,54 @@ sqrt_a(float x)
 	return r;
 }
 
-/* cell index of the fisheye map: floor((cbrt(asinh x) - B) / A), with
- * asinh and cbrt from log2/exp2; only the cell choice depends on it, the
- * fractional coordinate comes from the exact node table. */
+struct DystConst {
+	float B[3], iA[3];
+};
+
+/* threads per block at most (the kernels' launch bound): the stride of the
+ * per-thread cell cache in shared memory */
+constexpr int CELL_STRIDE = 256;
+
+/* Fractional logical coordinate on a fisheye axis, with the cell found
+ * exactly against the node table: the FP32 map only gives the first guess,
+ * node comparisons settle it (the answer depends on x and the table alone).
+ * The last interior cell of each thread is kept in `cache` (x0, x1,
+ * 1/(x1 - x0), i): a ray moves about 0.01 M per stage through cells 0.2-2 M
+ * wide, so nearly every call skips the map (three MUFU in a chain) and the
+ * two node loads, with the same result the search would give. */
 __device__ __forceinline__ float
-axis_uvw32(const GridParams &g, int a, float x, float Bf, float iAf)
+axis_uvw32c(const GridParams &g, int a, float x, float Bf, float iAf, float4 &cache)
 {
+	if(x >= cache.x && x < cache.y)
+		return cache.w + (x - cache.x) * cache.z;
 	const int n = a == 0 ? g.nx : a == 1 ? g.ny : g.nz;
+	const float *nd = g.nodes_f[a];
+	if(!(x >= __ldg(nd)))
+		return 0.0f;              /* before the first node (or NaN): clamp-to-edge */
+	if(x >= __ldg(nd + n - 1))
+		return (float)(n - 1);    /* at or past the last node */
 	float ax = fabsf(x);
 	float as = 0.69314718f * lg2_a(ax + sqrt_a(fmaf(ax, ax, 1.0f)));   /* asinh|x| */
 	float cb = as > 0.0f ? ex2_a(0.33333334f * lg2_a(as)) : 0.0f;       /* cbrt     */
 	cb = copysignf(cb, x);
 	float xi = floorf((cb - Bf) * iAf);
-	int i;
-	if(!(xi >= 0.0f))
-		i = 0;
-	else if(xi > (float)(n - 1))
-		i = n - 1;
-	else
-		i = (int)xi;
-	float x0 = __ldg(g.nodes_f[a] + i);
-	float x1 = __ldg(g.nodes_f[a] + i + 1);
-	float u  = (float)i + (x - x0) * rcp_a(x1 - x0);
-	u = fmaxf(u, 0.0f);
-	return fminf(u, (float)(n - 1));
+	int i = xi >= 0.0f ? (xi <= (float)(n - 2) ? (int)xi : n - 2) : 0;
+	float x0 = __ldg(nd + i), x1 = __ldg(nd + i + 1);
+	/* nd[0] <= x < nd[n-1] keeps both walks inside [0, n-2] */
+	for(int it = 0; it < 2 && x < x0; ++it) {
+		--i;
+		x1 = x0;
+		x0 = __ldg(nd + i);
+	}
+	for(int it = 0; it < 2 && x >= x1; ++it) {
+		++i;
+		x0 = x1;
+		x1 = __ldg(nd + i + 1);
+	}
+	const float inv = rcp_a(x1 - x0);
+	cache = make_float4(x0, x1, inv, (float)i);
+	return (float)i + (x - x0) * inv;
 }
-
-struct DystConst {
-	float B[3], iA[3];
-};
 
 /* eight consecutive floats from a 32-byte aligned address, through the
  * read-only path */
@@ -217,7 +236,7 @@ inside32(const GridParams &g, const float *q)
  * kn[0..3] and kn[4], contracted per corner like Gamma. */
 template <bool RT = false>
 __device__ __forceinline__ void
-dyst_rhs32(const GridParams &g, const DystConst &dc, const float *s, float *ds,
+dyst_rhs32(const GridParams &g, const DystConst &dc, float4 *cells, const float *s, float *ds,
            float *kn = nullptr)
 {
 	const float *u = s + 4;
@@ -235,7 +254,7 @@ dyst_rhs32(const GridParams &g, const DystConst &dc, const float *s, float *ds,
 	const int n[3] = {g.nx, g.ny, g.nz};
 #pragma unroll
 	for(int a = 0; a < 3; ++a) {
-		float uu = axis_uvw32(g, a, s[a + 1], dc.B[a], dc.iA[a]);
+		float uu = axis_uvw32c(g, a, s[a + 1], dc.B[a], dc.iA[a], cells[a * CELL_STRIDE]);
 		float fl = floorf(uu);
 		i0[a] = (int)fl;
 		w[a] = uu - fl;
@@ -341,6 +360,12 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 	constexpr int NR = 2 * NF;       /* FP64 transfer state           */
 	const unsigned FULL = 0xffffffffu;
 	const int lane = threadIdx.x & 31;
+	/* each thread's last cell per axis (axis_uvw32c); empty to start */
+	__shared__ float4 s_cells[3 * CELL_STRIDE];
+	float4 *cells = s_cells + threadIdx.x;
+#pragma unroll
+	for(int a = 0; a < 3; ++a)
+		cells[a * CELL_STRIDE] = make_float4(INFINITY, -INFINITY, 0.0f, 0.0f);
 	float hi[ND], lo[ND];
 	double rt[NR > 0 ? NR : 1];
 	long long ray = 0;
@@ -434,7 +459,7 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 #pragma unroll 1
 			for(int st = 0; st < 4; ++st) {
 				float kn[5];
-				dyst_rhs32<true>(g, dc, t, k, kn);
+				dyst_rhs32<true>(g, dc, cells, t, k, kn);
 				const double kd[4] = {kn[0], kn[1], kn[2], kn[3]};
 				rt_rhs_fast<NF>(c->tf, c->nu_hz, kd, (double)kn[4], trt + NF, krt, krt + NF);
 				const float wg = (st == 1 || st == 2) ? 2.0f : 1.0f;
@@ -456,25 +481,25 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 			for(int i = 0; i < NR; ++i)
 				rt[i] = fma(hsd / 6.0, srt[i], rt[i]);
 		} else {
-		dyst_rhs32(g, dc, hi, k);
+		dyst_rhs32(g, dc, cells, hi, k);
 #pragma unroll
 		for(int i = 0; i < ND; ++i) {
 			sum[i] = k[i];
 			t[i] = fmaf(hh, k[i], hi[i]);
 		}
-		dyst_rhs32(g, dc, t, k);
+		dyst_rhs32(g, dc, cells, t, k);
 #pragma unroll
 		for(int i = 0; i < ND; ++i) {
 			sum[i] = fmaf(2.0f, k[i], sum[i]);
 			t[i] = fmaf(hh, k[i], hi[i]);
 		}
-		dyst_rhs32(g, dc, t, k);
+		dyst_rhs32(g, dc, cells, t, k);
 #pragma unroll
 		for(int i = 0; i < ND; ++i) {
 			sum[i] = fmaf(2.0f, k[i], sum[i]);
 			t[i] = fmaf(hs, k[i], hi[i]);
 		}
-		dyst_rhs32(g, dc, t, k);
+		dyst_rhs32(g, dc, cells, t, k);
 		}
 		const float h6 = hs * (1.0f / 6.0f);
 		bool bad = false;
