@@ -36,7 +36,8 @@ enum gray_status {
 	GRAY_ECUDA     = -3,  /* CUDA runtime error                    */
 	GRAY_ENODEV    = -4,  /* no usable sm_100 device               */
 	GRAY_EBUDGET   = -5,  /* request exceeds the HBM budget        */
-	GRAY_ETIMEOUT  = -6,  /* bounded device wait ran out           */
+	GRAY_ETIMEOUT  = -6,  /* reserved: no kernel here waits on a
+	                         flag, so no entry point returns it     */
 	GRAY_ENOTFOUND = -7,  /* unknown render / request id           */
 	GRAY_ESTATE    = -8,  /* call out of order (e.g. no icond yet) */
 	GRAY_ESIZE     = -9,  /* host buffer size does not match       */
