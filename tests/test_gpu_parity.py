@@ -3,8 +3,8 @@
 FP64: the plain kernel and the oracle place every fused multiply-add
 identically and use IEEE divide/sqrt, so the geodesic agrees bit for bit;
 the torus transfer calls exp/pow, whose last bit may differ between CUDA
-and glibc.  Tolerance: 1e-10 relative per ray per component (north-star
-bar), with the bit-identical fraction reported.
+and glibc.  Tolerance: 1e-10 relative per ray per component (the FP64
+parity bar), with the bit-identical fraction reported.
 Mixed: FP32 bulk with FP64 islands; image (I_nu) relative L2 error vs the
 FP64 kernel <= 1e-4 per frequency.
 """
