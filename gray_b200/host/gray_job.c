@@ -412,6 +412,21 @@ gray_read_raw(const char *path, double *data, double *info, size_t n_data, size_
 	return st;
 }
 
+/* The dump layout the reference writes: sim-org/io.c:52-67 writes the
+ * device buffer as it is, so the element size is the run's precision
+ * (4 bytes for p=4, 8 for p=8) and the order is morder (AoS or SoA). */
+static size_t
+dump_size(const struct gray_job *j)
+{
+	return j->precision == 8 ? sizeof(double) : sizeof(float);
+}
+
+static int
+dump_layout(const struct gray_job *j)
+{
+	return strcmp(j->morder, "SoA") ? GRAY_LAYOUT_AOS : GRAY_LAYOUT_SOA;
+}
+
 /* Resume at dump i_init from the dump file a previous run wrote there
  * (the checkpoint the reference's dumps are but cannot load, io.c:37).
  * GRAY_ENOTFOUND when there is no such file: the run then starts from the
@@ -425,23 +440,32 @@ resume(struct gray_job *j, size_t i)
 	gray_job_desc(&j->super, &d);
 	const size_t n_rays = d.n_width * d.n_height;
 	const size_t n_data = 8 + 2 * (size_t)d.n_freq;
-	double *data = malloc(sizeof(double) * n_rays * n_data);
-	double *info = malloc(sizeof(double) * n_rays);
-	int st = (data && info) ? GRAY_OK : GRAY_ENOMEM;
+	const size_t n = n_rays * n_data, sz = dump_size(j);
+	char name[512];
+	snprintf(name, sizeof(name), j->outfile, (int)i);
+	FILE *f = fopen(name, "rb");
+	if(!f)
+		return GRAY_ENOTFOUND;
+	size_t hdr[4];
+	double *data = malloc(sizeof(double) * n);
+	void *raw = malloc(sz * n);
+	int st = (data && raw) ? GRAY_OK : GRAY_ENOMEM;
+	if(!st && (fread(hdr, sizeof(size_t), 4, f) != 4 || hdr[0] != sz || hdr[1] != n_data ||
+	           hdr[2] != d.n_width || hdr[3] != d.n_height || fread(raw, sz, n, f) != n))
+		st = GRAY_ESIZE;
+	fclose(f);
 	if(!st) {
-		char name[512];
-		snprintf(name, sizeof(name), j->outfile, (int)i);
-		st = gray_read_raw(name, data, info, n_data, d.n_width, d.n_height);
+		for(size_t k = 0; k < n; ++k)
+			data[k] = sz == sizeof(float) ? (double)((float *)raw)[k] : ((double *)raw)[k];
+		st = gray_write_state(j->ctx, j->render, data, sizeof(double) * n, dump_layout(j));
 	}
-	if(!st)
-		st = gray_write_state(j->ctx, j->render, data, sizeof(double) * n_rays * n_data,
-		                      GRAY_LAYOUT_AOS);
+	free(raw);
 	free(data);
-	free(info);
 	return st;
 }
 
-/* sim-org/io.c:39-72 dump(): state in AoS with its info diagnostic */
+/* sim-org/io.c:39-72 dump(): header {sz, n_data, W, H}, the state, its
+ * info diagnostic, in the run's element size and memory order */
 static int
 dump(struct gray_job *j, size_t i)
 {
@@ -451,16 +475,35 @@ dump(struct gray_job *j, size_t i)
 	gray_job_desc(&j->super, &d);
 	const size_t n_rays = d.n_width * d.n_height;
 	const size_t n_data = 8 + 2 * (size_t)d.n_freq;
-	double *data = malloc(sizeof(double) * n_rays * n_data);
+	const size_t n = n_rays * n_data, sz = dump_size(j);
+	double *data = malloc(sizeof(double) * n);
 	double *info = malloc(sizeof(double) * n_rays);
 	int st = (data && info) ? GRAY_OK : GRAY_ENOMEM;
 	if(!st)
-		st = gray_read_state(j->ctx, j->render, data, sizeof(double) * n_rays * n_data,
-		                     info, sizeof(double) * n_rays, GRAY_LAYOUT_AOS);
+		st = gray_read_state(j->ctx, j->render, data, sizeof(double) * n, info,
+		                     sizeof(double) * n_rays, dump_layout(j));
 	if(!st) {
 		char name[512];
 		snprintf(name, sizeof(name), j->outfile, (int)i);
-		st = gray_write_raw(name, data, info, n_data, d.n_width, d.n_height);
+		if(sz == sizeof(double)) {
+			st = gray_write_raw(name, data, info, n_data, d.n_width, d.n_height);
+		} else { /* p=4: the reference's state is float, so is its dump */
+			float *fd = malloc(sizeof(float) * (n + n_rays));
+			FILE *f = fd ? fopen(name, "wb") : NULL;
+			int ok = 0;
+			if(f) {
+				for(size_t k = 0; k < n; ++k)
+					fd[k] = (float)data[k];
+				for(size_t k = 0; k < n_rays; ++k)
+					fd[n + k] = (float)info[k];
+				const size_t hdr[4] = {sz, n_data, d.n_width, d.n_height};
+				ok = fwrite(hdr, sizeof(size_t), 4, f) == 4 &&
+				     fwrite(fd, sz, n + n_rays, f) == n + n_rays;
+				ok = (fclose(f) == 0) && ok;
+			}
+			st = fd ? (ok ? GRAY_OK : GRAY_EINVAL) : GRAY_ENOMEM;
+			free(fd);
+		}
 	}
 	free(data);
 	free(info);
