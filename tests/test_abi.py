@@ -72,3 +72,19 @@ def test_bench_h2d_bytes_match_the_render_table(tmp_path):
     sys.path.insert(0, ROOT)
     import bench
     assert bench.H2D_BYTES_PER_RENDER == size
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    """No CPU fallback: without libgray_cuda.so every entry point raises."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "from gray_b200 import api\n"
+            "api.LIB_PATH = %r\n"
+            "try:\n"
+            "    api.Context(0)\n"
+            "except RuntimeError as e:\n"
+            "    print('raised:', e)\n" % (ROOT, str(tmp_path / "absent.so")))
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert p.returncode == 0, p.stderr
+    assert "raised:" in p.stdout and "not built" in p.stdout
