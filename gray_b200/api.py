@@ -76,11 +76,13 @@ class RenderDesc(ctypes.Structure):
 
 class LaunchPlan(ctypes.Structure):
     _fields_ = [("block", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
-                ("rays_per_thread", ctypes.c_int32), ("ns", ctypes.c_double)]
+                ("rays_per_thread", ctypes.c_int32), ("rk4_rolled", ctypes.c_int32),
+                ("ns", ctypes.c_double)]
 
     def as_dict(self):
         return {"block": self.block, "blocks_per_sm": self.blocks_per_sm,
-                "rays_per_thread": self.rays_per_thread, "trial_ns": self.ns}
+                "rays_per_thread": self.rays_per_thread, "rk4_rolled": self.rk4_rolled,
+                "trial_ns": self.ns}
 
 
 class ServeConfig(ctypes.Structure):
@@ -456,8 +458,8 @@ class Context:
         _ck(lib().gray_plan(self.h, batch.id, flags, ctypes.byref(p)), "gray_plan")
         return p
 
-    def set_plan(self, block, blocks_per_sm=0, rays_per_thread=2):
-        p = LaunchPlan(block, blocks_per_sm, rays_per_thread, 0.0)
+    def set_plan(self, block, blocks_per_sm=0, rays_per_thread=2, rk4_rolled=0):
+        p = LaunchPlan(block, blocks_per_sm, rays_per_thread, rk4_rolled, 0.0)
         _ck(lib().gray_set_plan(self.h, ctypes.byref(p)), "gray_set_plan")
 
     def get_plan(self):

@@ -1210,7 +1210,7 @@ static bool
 same_cfg(const MixedLaunch &a, const MixedLaunch &b)
 {
 	return a.block == b.block && a.blocks_per_sm == b.blocks_per_sm && a.sms == b.sms &&
-	       a.rays_per_thread == b.rays_per_thread;
+	       a.rays_per_thread == b.rays_per_thread && a.rk4_rolled == b.rk4_rolled;
 }
 
 extern "C" int
@@ -1274,7 +1274,8 @@ gray_batch_steps(gray_ctx *c, int id, uint64_t *steps)
 static int
 check_plan(const gray_launch_plan *p)
 {
-	if(!p || (p->rays_per_thread != 1 && p->rays_per_thread != 2))
+	if(!p || (p->rays_per_thread != 1 && p->rays_per_thread != 2) ||
+	   (p->rk4_rolled != 0 && p->rk4_rolled != 1))
 		return GRAY_EINVAL;
 	const int maxb = p->rays_per_thread == 2 ? 128 : 256;
 	if(p->block < 32 || p->block > maxb || p->block % 32 || p->blocks_per_sm < 0)
@@ -1293,6 +1294,7 @@ gray_set_plan(gray_ctx *c, const gray_launch_plan *p)
 	c->mixed.block = p->block;
 	c->mixed.blocks_per_sm = p->blocks_per_sm;
 	c->mixed.rays_per_thread = p->rays_per_thread;
+	c->mixed.rk4_rolled = p->rk4_rolled;
 	return GRAY_OK;
 }
 
@@ -1304,12 +1306,13 @@ gray_get_plan(const gray_ctx *c, gray_launch_plan *p)
 	p->block = c->mixed.block;
 	p->blocks_per_sm = c->mixed.blocks_per_sm;
 	p->rays_per_thread = c->mixed.rays_per_thread;
+	p->rk4_rolled = c->mixed.rk4_rolled;
 	p->ns = 0.0;
 	return GRAY_OK;
 }
 
 /* Candidates: rays per thread {2, 1} x block {64, 128(, 256)} x blocks per
- * SM {all that fit, half of them}.  Each is timed (best of two) over the
+ * SM {all that fit, half of them} x RK4 stages {unrolled, looped}.  Each is timed (best of two) over the
  * first two dump intervals of every render in the batch, launched directly
  * (not through the graph). */
 extern "C" int
@@ -1324,7 +1327,7 @@ gray_plan(gray_ctx *c, int id, int flags, gray_launch_plan *best)
 	if(flags == GRAY_PLAN_ESTIMATE || b->spacetime == GRAY_ST_NUMERICAL) {
 		/* the rule: 256 threads, one ray each (the numerical kernel has
 		 * only this shape) */
-		c->mixed = MixedLaunch{256, 0, c->sms, 1};
+		c->mixed = MixedLaunch{256, 0, c->sms, 1, 0};
 		return gray_get_plan(c, best);
 	}
 	/* trial table: the first two dump intervals of every render */
@@ -1339,20 +1342,21 @@ gray_plan(gray_ctx *c, int id, int flags, gray_launch_plan *best)
 	CK(cudaMemcpyAsync(b->d_table, trial.data(), trial.size() * sizeof(MixedRender),
 	                   cudaMemcpyHostToDevice, c->stream));
 	MixedTable T = batch_table(b);
-	MixedLaunch cand[16];
+	MixedLaunch cand[32];
 	int nc = 0;
-	for(int rpt = 2; rpt >= 1; --rpt)
-		for(int blk = 64; blk <= (rpt == 2 ? 128 : 256); blk *= 2) {
-			MixedLaunch m = {blk, 0, c->sms, rpt};
-			int occ = 0;
-			if(mixed_occupancy(b->n_freq, m, &occ) != cudaSuccess || occ <= 0)
-				continue;
-			cand[nc++] = m;
-			if(occ >= 2) {
-				m.blocks_per_sm = occ / 2;
+	for(int rolled = 0; rolled <= 1; ++rolled)
+		for(int rpt = 2; rpt >= 1; --rpt)
+			for(int blk = 64; blk <= (rpt == 2 ? 128 : 256); blk *= 2) {
+				MixedLaunch m = {blk, 0, c->sms, rpt, rolled};
+				int occ = 0;
+				if(mixed_occupancy(b->n_freq, m, &occ) != cudaSuccess || occ <= 0)
+					continue;
 				cand[nc++] = m;
+				if(occ >= 2) {
+					m.blocks_per_sm = occ / 2;
+					cand[nc++] = m;
+				}
 			}
-		}
 	double best_ns = 1e300;
 	MixedLaunch best_cfg = c->mixed;
 	int st = GRAY_OK;

@@ -92,6 +92,7 @@ struct MixedLaunch {
 	int blocks_per_sm;/* 0: from the occupancy calculator               */
 	int sms;
 	int rays_per_thread; /* 1 or 2 (analytic kernel only)               */
+	int rk4_rolled;      /* 0: RK4 stages unrolled; 1: one stage body looped */
 };
 
 /* numerical spacetime */

@@ -447,7 +447,7 @@ ticks(const Slot &S, int k, const V *hi, const V *lo)
 	return dh < S.n - S.h ? dh : S.n - S.h;
 }
 
-template <int NF, typename V>
+template <int NF, typename V, bool ROLLED>
 __global__ void __launch_bounds__(Lanes<V>::N == 1 ? 256 : 128)
 mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
              unsigned long long *__restrict__ steps)
@@ -553,7 +553,35 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 		for(int k = 0; k < L; ++k)
 			setl(hs, k, (float)dh[k] * S[k].dtn);
 		const V hh = bc<V>(0.5f) * hs;
-		{
+		if constexpr(ROLLED) {
+			/* one RHS body, looped over the stages (less code, same
+			 * arithmetic) */
+			V kk[ND], t[ND], sum[ND];
+#pragma unroll
+			for(int i = 0; i < ND; ++i)
+				t[i] = hi[i];
+#pragma unroll 1
+			for(int st = 0; st < 4; ++st) {
+				rhs<V, NF>(rc, t, kk);
+				const V wg = bc<V>((st == 1 || st == 2) ? 2.0f : 1.0f);
+				const V cg = st < 2 ? hh : hs;
+#pragma unroll
+				for(int i = 0; i < ND; ++i) {
+					if(st < 3)
+						sum[i] = st == 0 ? kk[i] : fmav(wg, kk[i], sum[i]);
+					t[i] = fmav(cg, kk[i], hi[i]);
+				}
+			}
+			const V h6 = hs * bc<V>(1.0f / 6.0f);
+#pragma unroll
+			for(int i = 0; i < ND; ++i) {
+				V inc = h6 * (sum[i] + kk[i]);
+				V yv = inc - lo[i];
+				V tv = hi[i] + yv;
+				lo[i] = (tv - hi[i]) - yv;
+				hi[i] = tv;
+			}
+		} else {
 			V kk[ND], t[ND], sum[ND];
 			rhs<V, NF>(rc, hi, kk);
 #pragma unroll
@@ -610,7 +638,7 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 		atomicAdd(steps, cnt);
 }
 
-template <int NF, typename V>
+template <int NF, typename V, bool ROLLED>
 cudaError_t
 launch_nf(const MixedTable &T, unsigned int *queue, unsigned long long *steps,
           cudaStream_t st, const MixedLaunch &cfg)
@@ -621,8 +649,8 @@ launch_nf(const MixedTable &T, unsigned int *queue, unsigned long long *steps,
 		return cudaErrorInvalidValue;
 	int per_sm = cfg.blocks_per_sm;
 	int occ = 0;
-	cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mixed_kernel<NF, V>,
-	                                                              block, 0);
+	cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+		&occ, mixed_kernel<NF, V, ROLLED>, block, 0);
 	if(e != cudaSuccess)
 		return e;
 	if(per_sm <= 0 || per_sm > occ)
@@ -633,7 +661,7 @@ launch_nf(const MixedTable &T, unsigned int *queue, unsigned long long *steps,
 	unsigned grid = (unsigned)(want < need ? want : need);
 	if(grid == 0)
 		grid = 1;
-	mixed_kernel<NF, V><<<grid, block, 0, st>>>(T, queue, steps);
+	mixed_kernel<NF, V, ROLLED><<<grid, block, 0, st>>>(T, queue, steps);
 	return cudaGetLastError();
 }
 
@@ -642,25 +670,31 @@ cudaError_t
 launch_v(const MixedTable &T, int n_freq, unsigned int *queue, unsigned long long *steps,
          cudaStream_t st, const MixedLaunch &cfg)
 {
+#define LNF(NF) (cfg.rk4_rolled ? launch_nf<NF, V, true>(T, queue, steps, st, cfg) \
+                                : launch_nf<NF, V, false>(T, queue, steps, st, cfg))
 	switch(n_freq) {
-	case 0: return launch_nf<0, V>(T, queue, steps, st, cfg);
-	case 1: return launch_nf<1, V>(T, queue, steps, st, cfg);
-	case 2: return launch_nf<2, V>(T, queue, steps, st, cfg);
-	case 3: return launch_nf<3, V>(T, queue, steps, st, cfg);
-	case 4: return launch_nf<4, V>(T, queue, steps, st, cfg);
-	case 5: return launch_nf<5, V>(T, queue, steps, st, cfg);
-	case 6: return launch_nf<6, V>(T, queue, steps, st, cfg);
-	case 7: return launch_nf<7, V>(T, queue, steps, st, cfg);
-	case 8: return launch_nf<8, V>(T, queue, steps, st, cfg);
+	case 0: return LNF(0);
+	case 1: return LNF(1);
+	case 2: return LNF(2);
+	case 3: return LNF(3);
+	case 4: return LNF(4);
+	case 5: return LNF(5);
+	case 6: return LNF(6);
+	case 7: return LNF(7);
+	case 8: return LNF(8);
 	default: return cudaErrorInvalidValue;
 	}
+#undef LNF
 }
 
 template <int NF, typename V>
 cudaError_t
-occ_nf(int block, int *out)
+occ_nf(int block, bool rolled, int *out)
 {
-	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, mixed_kernel<NF, V>, block, 0);
+	return rolled ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+	                    out, mixed_kernel<NF, V, true>, block, 0)
+	              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+	                    out, mixed_kernel<NF, V, false>, block, 0);
 }
 
 } /* namespace */
@@ -682,7 +716,8 @@ mixed_occupancy(int n_freq, const MixedLaunch &cfg, int *blocks_per_sm)
 {
 	const bool two = cfg.rays_per_thread == 2;
 	const int block = cfg.block > 0 ? cfg.block : (two ? 128 : 256);
-#define OCC(NF) (two ? occ_nf<NF, F2>(block, blocks_per_sm) : occ_nf<NF, float>(block, blocks_per_sm))
+#define OCC(NF) (two ? occ_nf<NF, F2>(block, cfg.rk4_rolled, blocks_per_sm) \
+                     : occ_nf<NF, float>(block, cfg.rk4_rolled, blocks_per_sm))
 	switch(n_freq) {
 	case 0: return OCC(0);
 	case 1: return OCC(1);

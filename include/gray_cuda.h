@@ -217,6 +217,8 @@ typedef struct gray_launch_plan {
 	int32_t block;            /* threads per block                          */
 	int32_t blocks_per_sm;    /* 0 = as many as fit                         */
 	int32_t rays_per_thread;  /* 1 (scalar FP32) or 2 (packed f32x2)         */
+	int32_t rk4_rolled;       /* 0: the four RK4 stages unrolled (one RHS
+	                             body each), 1: one RHS body in a loop     */
 	double  ns;               /* measured trial time (gray_plan output)      */
 } gray_launch_plan;
 
@@ -227,7 +229,8 @@ enum gray_plan_flags {
 
 /* Autotuner replacing the lux planner of sim/gray/Kerr/ocl.c:41-75 and
  * tests/ck_sample.c:84-104 (7 work-group sizes, estimate or measure): picks
- * block size, blocks per SM and rays per thread for the batch's kernel,
+ * block size, blocks per SM, rays per thread and RK4 stage unrolling for
+ * the batch's kernel,
  * installs it in the context and returns it.  MEASURE runs trial launches
  * over the first dump intervals of the batch, leaving the renders' state
  * undefined (gray_batch_run / gray_run start from icond again). */

@@ -48,6 +48,8 @@ def test_batch_equals_renders_alone(ctx):
 
 
 def test_rays_per_thread_variants_agree(ctx):
+    """Packed two-ray and scalar kernels, RK4 stages unrolled or looped: the
+    looped stages run the same operations in the same order."""
     cfgs = small_survey(n=3)
     old = ctx.get_plan()
     try:
@@ -55,11 +57,19 @@ def test_rays_per_thread_variants_agree(ctx):
         two = [alone(ctx, c)[0] for c in cfgs]
         ctx.set_plan(256, 0, 1)
         one = [alone(ctx, c)[0] for c in cfgs]
+        ctx.set_plan(256, 0, 1, rk4_rolled=1)
+        rolled = [alone(ctx, c)[0] for c in cfgs]
+        ctx.set_plan(128, 0, 2, rk4_rolled=1)
+        two_rolled = [alone(ctx, c)[0] for c in cfgs]
     finally:
-        ctx.set_plan(old.block, old.blocks_per_sm, old.rays_per_thread)
+        ctx.set_plan(old.block, old.blocks_per_sm, old.rays_per_thread, old.rk4_rolled)
     for a, b in zip(one, two):
         img = np.linalg.norm(a[:, 8:12] - b[:, 8:12]) / np.linalg.norm(b[:, 8:12])
         assert img <= 1e-5, img
+    for a, b in list(zip(one, rolled)) + list(zip(two, two_rolled)):
+        assert rel(b, a) <= 1e-6
+    print("looped RK4 bit-identical to unrolled: %s" %
+          all(np.array_equal(a, b) for a, b in zip(one, rolled)))
 
 
 def test_plan_measures_and_installs(ctx):
@@ -70,14 +80,16 @@ def test_plan_measures_and_installs(ctx):
     try:
         p = ctx.plan(b, api.PLAN_MEASURE)
         assert p.rays_per_thread in (1, 2) and p.block % 32 == 0 and p.ns > 0
+        assert p.rk4_rolled in (0, 1)
         cur = ctx.get_plan()
-        assert (cur.block, cur.rays_per_thread) == (p.block, p.rays_per_thread)
+        assert (cur.block, cur.rays_per_thread, cur.rk4_rolled) == \
+            (p.block, p.rays_per_thread, p.rk4_rolled)
         b.run()
         for r, c in zip(rs, cfgs):
             d, _ = alone(ctx, c)
             assert rel(r.state(api.LAYOUT_AOS)[0], d) <= 1e-5
     finally:
-        ctx.set_plan(old.block, old.blocks_per_sm, old.rays_per_thread)
+        ctx.set_plan(old.block, old.blocks_per_sm, old.rays_per_thread, old.rk4_rolled)
         b.close()
         for r in rs:
             r.close()
