@@ -230,7 +230,8 @@ inside32(const GridParams &g, const float *q)
 }
 
 /* Gamma^mu_ab u^a u^b for mu = t,x,y,z from the 40 interpolated Gamma:
- * corner rows are gathered as float4 and accumulated in f32x2 pairs.
+ * each corner's row is gathered with 32-byte loads and contracted with
+ * u^a u^b before the trilinear weight is applied.
  * With RT, also the covariant momentum k_mu = g_mu,nu u^nu (dyst.cl:55-81,
  * with the g_zz flag of dyst.cl:78) and n_e = rho (flow.cl:48) into
  * kn[0..3] and kn[4], contracted per corner like Gamma. */
