@@ -15,7 +15,8 @@
  *                           n_electron:ne beta_crit:bc R_high:Rh R_low:Rl nu
  * plus the options of the analytic torus (flow, torus_n0, torus_kappa,
  * torus_hr), of the thermal flow (flow_te:te, flow_b:b; flow.cl:51-52 fixes
- * them at 1e12 and 0) and the stop rule (term).  conf() follows the lux convention:
+ * them at 1e12 and 0), the stop rule (term) and the launch planner (plan:pl,
+ * measure or estimate).  conf() follows the lux convention:
  * 0 when the argument was consumed (sim/gray.c:37-73).
  *
  * init() replaces sim/gray.c:75-151 (device, ray buffer, initcond, planner);
@@ -70,6 +71,7 @@ struct gray_job {
 	double   torus_n0, torus_kappa, torus_hr;
 	double   flow_te, flow_b;
 	char     term[16];
+	char     plan[16];
 
 	/* run time */
 	gray_ctx *ctx;
@@ -130,6 +132,7 @@ static const opt OPTS[] = {
 	{"torus_hr",             T_DBL,  OFF(torus_hr), SZ(torus_hr), "0.3"},
 	{"flow_te:te",           T_DBL,  OFF(flow_te), SZ(flow_te), "1e12"},
 	{"flow_b:b",             T_DBL,  OFF(flow_b), SZ(flow_b), "0"},
+	{"plan:pl",              T_STR,  OFF(plan), SZ(plan), "measure"},
 	{"term",                 T_STR,  OFF(term), SZ(term), "eps"},
 };
 #define N_OPTS (sizeof(OPTS) / sizeof(OPTS[0]))
@@ -267,6 +270,8 @@ valid_choices(const struct gray_job *j)
 	if(strcmp(j->flow, "torus") && strcmp(j->flow, "none"))
 		return 0;
 	if(strcmp(j->term, "eps") && strcmp(j->term, "rplus"))
+		return 0;
+	if(strcmp(j->plan, "measure") && strcmp(j->plan, "estimate"))
 		return 0;
 	return 1;
 }
@@ -523,6 +528,21 @@ init(gray_lux_job *ego)
 	st = gray_render_create(EGO->ctx, &d, &EGO->render);
 	if(st)
 		return st;
+	/* the lux planner of sim/gray/Kerr/ocl.c:41-75: time the launch shapes
+	 * on this render (a mixed one: the FP64 kernel has a single shape);
+	 * exec starts from icond, so the trial launches leave no trace */
+	if(d.precision == GRAY_PREC_MIXED && !strcmp(EGO->plan, "measure")) {
+		int batch;
+		gray_launch_plan best;
+		if((st = gray_batch_create(EGO->ctx, &EGO->render, 1, &batch)))
+			return st;
+		st = gray_plan(EGO->ctx, batch, GRAY_PLAN_MEASURE, &best);
+		gray_batch_destroy(EGO->ctx, batch);
+		if(st)
+			return st;
+		printf("GRay2:init: plan: block %d, rays/thread %d, RK4 %s\n", best.block,
+		       best.rays_per_thread, best.rk4_rolled ? "looped" : "unrolled");
+	}
 	EGO->steps = 0;
 	EGO->ns = 0.0;
 	return GRAY_OK;
