@@ -12,7 +12,9 @@
  *    approximate rcp/rsqrt/ex2/lg2 instructions in place of IEEE divide and
  *    square-root sequences; with two rays per thread the whole step runs in
  *    sm_100 packed f32x2 arithmetic (one FFMA2/FMUL2/FADD2 issue slot serves
- *    both rays);
+ *    both rays), and with one ray per thread the RK4 stage sums, stage
+ *    states and compensated update run on pairs of state components in
+ *    the same packed arithmetic;
  *  - FP64 is kept where it matters: the state update is compensated (Kahan
  *    hi + lo pairs of FP32), the Kerr-Schild radius root (KS.cl:48-55) is
  *    evaluated in FP64 near the horizon where the stop rule and step-size
@@ -97,6 +99,21 @@ __device__ __forceinline__ F2 operator-(F2 a, F2 b)
 	return r;
 }
 __device__ __forceinline__ F2 operator-(F2 a) { F2 r; r.v = __fmul2_rn(a.v, make_float2(-1.0f, -1.0f)); return r; }
+
+/* a - b in one packed instruction (there is no __fsub2_rn intrinsic) */
+__device__ __forceinline__ float2
+sub2(float2 a, float2 b)
+{
+	float2 r;
+	asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
+	    "mov.b64 ra, {%2, %3};\n\t"
+	    "mov.b64 rb, {%4, %5};\n\t"
+	    "sub.rn.f32x2 rd, ra, rb;\n\t"
+	    "mov.b64 {%0, %1}, rd;\n\t}"
+	    : "=f"(r.x), "=f"(r.y)
+	    : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+	return r;
+}
 
 __device__ __forceinline__ float fmav(float a, float b, float c) { return fmaf(a, b, c); }
 __device__ __forceinline__ F2 fmav(F2 a, F2 b, F2 c) { F2 r; r.v = __ffma2_rn(a.v, b.v, c.v); return r; }
@@ -580,6 +597,61 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 				V tv = hi[i] + yv;
 				lo[i] = (tv - hi[i]) - yv;
 				hi[i] = tv;
+			}
+		} else if constexpr(L == 1) {
+			/* the same stages with the bookkeeping on component pairs
+			 * (2j, 2j+1; ND is even): each stage sum, stage state and
+			 * compensated update is one packed f32x2 instruction per
+			 * pair.  The operations and roundings are those of the
+			 * lane-wise form below, except that a product feeding an
+			 * add is not contracted into an FMA here */
+			constexpr int NP = ND / 2;
+			V kk[ND], t[ND];
+			float2 H[NP], S2[NP];
+			const float2 hh2 = make_float2(hh, hh), hs2 = make_float2(hs, hs);
+			const float2 two2 = make_float2(2.0f, 2.0f);
+#pragma unroll
+			for(int j = 0; j < NP; ++j)
+				H[j] = make_float2(hi[2 * j], hi[2 * j + 1]);
+			rhs<V, NF>(rc, hi, kk);
+#pragma unroll
+			for(int j = 0; j < NP; ++j) {
+				S2[j] = make_float2(kk[2 * j], kk[2 * j + 1]);
+				const float2 s = __ffma2_rn(hh2, S2[j], H[j]);
+				t[2 * j] = s.x;
+				t[2 * j + 1] = s.y;
+			}
+			rhs<V, NF>(rc, t, kk);
+#pragma unroll
+			for(int j = 0; j < NP; ++j) {
+				const float2 K = make_float2(kk[2 * j], kk[2 * j + 1]);
+				S2[j] = __ffma2_rn(two2, K, S2[j]);
+				const float2 s = __ffma2_rn(hh2, K, H[j]);
+				t[2 * j] = s.x;
+				t[2 * j + 1] = s.y;
+			}
+			rhs<V, NF>(rc, t, kk);
+#pragma unroll
+			for(int j = 0; j < NP; ++j) {
+				const float2 K = make_float2(kk[2 * j], kk[2 * j + 1]);
+				S2[j] = __ffma2_rn(two2, K, S2[j]);
+				const float2 s = __ffma2_rn(hs2, K, H[j]);
+				t[2 * j] = s.x;
+				t[2 * j + 1] = s.y;
+			}
+			rhs<V, NF>(rc, t, kk);
+			const float2 h62 = make_float2(hs * (1.0f / 6.0f), hs * (1.0f / 6.0f));
+#pragma unroll
+			for(int j = 0; j < NP; ++j) {
+				const float2 K   = make_float2(kk[2 * j], kk[2 * j + 1]);
+				const float2 inc = __fmul2_rn(h62, __fadd2_rn(S2[j], K));
+				const float2 yv  = sub2(inc, make_float2(lo[2 * j], lo[2 * j + 1]));
+				const float2 tv  = __fadd2_rn(H[j], yv);
+				const float2 c   = sub2(sub2(tv, H[j]), yv);
+				hi[2 * j] = tv.x;
+				hi[2 * j + 1] = tv.y;
+				lo[2 * j] = c.x;
+				lo[2 * j + 1] = c.y;
 			}
 		} else {
 			V kk[ND], t[ND], sum[ND];
