@@ -118,6 +118,34 @@ def test_schwarzschild_capture_threshold():
         assert (r < 2.1) == captured, (b, r)
 
 
+def far_field_deviation(r_obs):
+    """Rays of a camera at r_obs over 1000 M of affine parameter: the
+    relative departure of q from the straight line q0 + u0 dl, and of u from
+    u0 (maxima over 16 rays)."""
+    cfg = dict(a_spin=0.9, w_img=0.2 * r_obs, h_img=0.2 * r_obs, r_obs=r_obs, i_obs=60.0,
+               j_obs=0.0, n_width=4, n_height=4, t_init=0.0, dt_dump=-250.0, n_sub=1000,
+               n_dump=4, nu=())
+    rays = np.arange(16)
+    s0 = O.icond(cfg, rays)
+    s1, _, steps = O.trace(cfg, rays, nthreads=1)
+    dl = cfg["n_dump"] * cfg["dt_dump"]
+    line = s0[:, :4] + s0[:, 4:8] * dl
+    dq = np.linalg.norm(s1[:, :4] - line, axis=1) / np.linalg.norm(s0[:, 4:8] * dl, axis=1)
+    du = np.linalg.norm(s1[:, 4:8] - s0[:, 4:8], axis=1) / np.linalg.norm(s0[:, 4:8], axis=1)
+    assert np.all(steps == 4 * 1000)
+    return dq.max(), du.max()
+
+
+def test_large_r_straight_line_limit():
+    """Far from the hole the Christoffel symbols fall off as M / r^2: rays
+    are straight lines, and their departure from one scales as r^-2."""
+    q4, u4 = far_field_deviation(1e4)
+    q5, u5 = far_field_deviation(1e5)
+    assert q5 < 1e-6 and u5 < 1e-6
+    assert 70.0 < q4 / q5 < 140.0, (q4, q5)
+    assert 70.0 < u4 / u5 < 140.0, (u4, u5)
+
+
 def test_getdt_rule():
     """phys.cl:48-64: stop below eps 0.01; else min(|dt|, 0.01 eps^2)."""
     cfg = dict(a_spin=0.9)
