@@ -122,7 +122,8 @@ gray_run_mixed_noalloc(int device, const gray_render_desc *descs, int n_renders,
 	if(e == cudaSuccess)
 		e = cudaMemcpyAsync(S->prefix, prefix, sizeof(unsigned long long) * n_renders,
 		                    cudaMemcpyHostToDevice, st);
-	/* the array keeps the last call's contents: the counters restart at 0 */
+	/* the array keeps the last call's contents: the step counter restarts
+	 * at 0 here, the ray queue in launch_mixed_table */
 	if(e == cudaSuccess)
 		e = cudaMemsetAsync(&S->steps, 0, sizeof(S->steps), st);
 	if(e == cudaSuccess) {
