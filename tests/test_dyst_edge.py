@@ -1,6 +1,7 @@
 """Edge cases of the numerical-spacetime path against the CPU oracle: an
 anisotropic grid over an asymmetric box, a single time level, linear time
-extrapolation far outside [t1, t2] (reference semantics), and the thermal
+extrapolation far outside [t1, t2] (reference semantics), forward tracing
+(dt_dump > 0, out past t2 and the box edge), and the thermal
 transfer with the g_zz flag.  FP64 geodesics bit-identical; the transfer
 within the 1e-10 parity bar; mixed end positions within 1e-3 (L2) of FP64
 on the rays that leave the box (physics mode)."""
@@ -22,6 +23,7 @@ CASES = {
     "anisotropic_physics": (0.0, 5.0, True, False, dict(r_obs=80.0, dt_dump=-10.0, n_dump=24)),
     "single_level": (3.0, 3.0, False, False, dict(r_obs=25.0, dt_dump=-2.0, n_dump=3)),
     "time_extrapolation": (0.0, 2.0, False, False, dict(r_obs=25.0, dt_dump=-3.0, n_dump=4)),
+    "forward": (0.0, 5.0, False, False, dict(r_obs=25.0, dt_dump=2.0, n_dump=3)),
     "thermal_gzz": (0.0, 5.0, True, True, dict(r_obs=80.0, dt_dump=-10.0, n_dump=24,
                                                 nu=(1e10, 3e11), flow_te=10.0, flow_b=1e3)),
 }

@@ -27,6 +27,13 @@ def test_schedule_of_a_backward_run():
     assert first == 3 and list(ref) == list(pairs)
 
 
+def test_schedule_of_a_forward_run():
+    pairs = api.series_schedule(TIMES, -20.0, 2.0, 9)
+    assert list(pairs) == [0, 0, 0, 1, 1, 1, 2, 2, 3]
+    first, ref = O.series_schedule(TIMES, -20.0, 2.0, 9)
+    assert first == 0 and list(ref) == list(pairs)
+
+
 def test_schedule_frozen_and_rejected():
     assert list(api.series_schedule([7.0], 3.0, -1.0, 4)) == [0, 0, 0, 0]
     # fast light freezes the snapshot of the pair bracketing t_init ([-10, -5])
@@ -102,6 +109,25 @@ def test_fp64_series_matches_oracle(ctx, snaps, physics):
                                        physics=physics, fast_light=True)
     assert np.max(np.abs(frozen[fin, 1:4] - ref[fin, 1:4])) > 1e-6
     print("series fp64 physics=%s: %d loads, %.2f ms" % (physics, loads, ns * 1e-6))
+
+
+@pytest.mark.gpu
+def test_fp64_forward_series_matches_oracle(ctx, snaps):
+    """Forward in time from the first snapshot: the levels advance upward."""
+    c = cfg(r_obs=30.0, t_init=-20.0, dt_dump=2.0)
+    grid = api.make_grid(N, -BOX, BOX)
+    r = ctx.render(dict(c, precision=api.PREC_FP64))
+    try:
+        _, loads = r.run_series(grid, TIMES, lambda k: snaps[k])
+        got, _ = r.state(api.LAYOUT_AOS)
+        steps = r.steps()
+    finally:
+        r.close()
+    assert loads == 5
+    ref, _, rsteps = O.dyst_series_trace(c, snaps, TIMES, -BOX, BOX, np.arange(48))
+    assert steps == rsteps.sum()
+    fin = np.all(np.isfinite(ref), axis=1)
+    assert fin.mean() > 0.5 and np.array_equal(got[fin], ref[fin])
 
 
 @pytest.mark.gpu
