@@ -127,14 +127,16 @@ iterate(Server *S, std::vector<Request *> &fresh)
 			continue;
 		}
 		r->d_info = r->d_data + (size_t)r->p.n_rays * r->p.n_data;
+		r->next_dump = 0;
+		/* in flight before its first launch, so that a failure below frees
+		 * it with the rest (the capacity was reserved at start) */
+		S->inflight.push_back(r);
 		cudaStream_t st_ = S->s[r->group() >= NUM_GROUP ? 1 : 0];
 		e = r->group() >= NUM_GROUP
 		        ? launch_dyst_icond(r->p, c->grid->gp, r->d_data, r->d_info, st_)
 		        : launch_icond64(r->p, r->d_data, r->d_info, st_);
 		if(e != cudaSuccess)
 			return gi_from_cuda(e);
-		r->next_dump = 0;
-		S->inflight.push_back(r);
 	}
 	if(S->inflight.empty())
 		return GRAY_OK;
@@ -302,11 +304,22 @@ loop(Server *S)
 			S->thread_status = st;
 			for(Request *r : S->inflight) {
 				release(S, r);
+				if(r->state != GRAY_REQ_RUNNING)
+					continue; /* retired (done or cancelled) before the failure */
 				r->state = GRAY_REQ_FAILED;
 				r->status = st;
 				S->stats.failed++;
 			}
 			S->inflight.clear();
+			/* admitted this iteration but not reached before the failure */
+			for(Request *r : fresh) {
+				if(r->state != GRAY_REQ_RUNNING)
+					continue;
+				S->inflight_bytes -= r->bytes;
+				r->state = GRAY_REQ_FAILED;
+				r->status = st;
+				S->stats.failed++;
+			}
 			for(Request *r : S->pending) {
 				r->state = GRAY_REQ_FAILED;
 				r->status = st;
@@ -424,6 +437,7 @@ gray_serve_start(gray_ctx *c, const gray_serve_config *cfg)
 	}
 	c->server = S;
 	try {
+		S->inflight.reserve(n); /* admission never grows it past this */
 		S->th = std::thread(loop, S);
 	} catch(...) {
 		c->server = nullptr;
