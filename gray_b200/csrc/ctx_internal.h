@@ -52,6 +52,9 @@ struct Batch {
 	cudaGraphExec_t exec = nullptr;
 	MixedLaunch graph_cfg = {0, 0, 0, 0};
 	cudaStream_t graph_stream = nullptr;
+	/* numerical batches: the grid parameters the graph's launches were
+	 * captured with (level pointers, time box, node tables) */
+	GridParams graph_gp;
 };
 
 struct Server; /* serve.cu */

@@ -1222,7 +1222,12 @@ gray_batch_run(gray_ctx *c, int id, double *ns)
 	if(b->spacetime == GRAY_ST_NUMERICAL && !grid_ready(c))
 		return GRAY_ESTATE;
 	CK(cudaSetDevice(c->device));
-	if(b->exec && (!same_cfg(b->graph_cfg, c->mixed) || b->graph_stream != c->stream))
+	/* the graph holds its launches' arguments: recapture when the launch
+	 * plan, the stream or (numerical) the grid it read has changed since,
+	 * e.g. after gray_swap_levels, a series run or a reshaped grid */
+	if(b->exec && (!same_cfg(b->graph_cfg, c->mixed) || b->graph_stream != c->stream ||
+	               (b->spacetime == GRAY_ST_NUMERICAL &&
+	                memcmp(&b->graph_gp, &c->grid->gp, sizeof(GridParams)) != 0)))
 		drop_graph(b);
 	if(!b->exec) {
 		/* capture once; the graph is replayed by every later run */
@@ -1245,6 +1250,8 @@ gray_batch_run(gray_ctx *c, int id, double *ns)
 		}
 		b->graph_cfg = c->mixed;
 		b->graph_stream = c->stream;
+		if(b->spacetime == GRAY_ST_NUMERICAL)
+			memcpy(&b->graph_gp, &c->grid->gp, sizeof(GridParams));
 	}
 	int st = timed_begin(c);
 	if(st)

@@ -146,3 +146,47 @@ def test_mixed_dyst_close_to_fp64(ctx):
     mom = np.linalg.norm(gmx[ok, 4:8] - g64[ok, 4:8]) / np.linalg.norm(g64[ok, 4:8])
     print("mixed vs fp64 dyst: pos %.3e mom %.3e, steps %d vs %d" % (pos, mom, smx, s64))
     assert pos <= 1e-4 and mom <= 1e-3
+
+
+@pytest.mark.gpu
+def test_numerical_batch_follows_grid_changes(ctx):
+    """A batch replays a captured graph; after the grid's levels change
+    (here gray_swap_levels) its next run must read the levels as they are
+    now, like renders run alone."""
+    small_grid(ctx, 16, 0.0, 5.0, False)
+    base = dict(a_spin=0.0, r_obs=25.0, i_obs=50.0, j_obs=20.0, w_img=20.0, h_img=20.0,
+                n_width=6, n_height=5, dt_dump=-2.0, n_dump=3, n_sub=50,
+                spacetime=api.ST_NUMERICAL, precision=api.PREC_MIXED)
+    cfgs = [base, dict(base, i_obs=70.0, n_width=4)]
+
+    def alone():
+        out = []
+        for c in cfgs:
+            r = ctx.render(c)
+            try:
+                r.run()
+                out.append(r.state(api.LAYOUT_AOS)[0])
+            finally:
+                r.close()
+        return out
+
+    rs = [ctx.render(c) for c in cfgs]
+    b = ctx.batch(rs)
+    try:
+        before = alone()
+        for _ in range(2):  # capture, then replay
+            b.run()
+            for r, d in zip(rs, before):
+                close_with_nans(r.state(api.LAYOUT_AOS)[0], d, 1e-10)
+        ctx.swap_levels()  # same buffers, exchanged: a different spacetime
+        after = alone()
+        assert any(np.nanmax(np.abs(a - d)) > 1e-6 for a, d in zip(after, before))
+        for _ in range(2):
+            b.run()
+            for r, d in zip(rs, after):
+                close_with_nans(r.state(api.LAYOUT_AOS)[0], d, 1e-10)
+    finally:
+        ctx.swap_levels()
+        b.close()
+        for r in rs:
+            r.close()
