@@ -256,6 +256,32 @@ set_opt(struct gray_job *j, const opt *o, const char *val)
 	return GRAY_EINVAL;
 }
 
+/* A file-name pattern takes at most one integer conversion, the dump index
+ * (sim-org/io.c formats the name with it); any other conversion would make
+ * snprintf read an argument that is not there. */
+static int
+valid_pattern(const char *s)
+{
+	int conv = 0;
+	for(const char *p = s; *p; ++p) {
+		if(*p != '%')
+			continue;
+		++p; /* the character after '%' */
+		if(*p == '%')
+			continue; /* a literal percent sign */
+		while(*p && strchr("-+ #0", *p))
+			++p;
+		while(*p >= '0' && *p <= '9')
+			++p;
+		if(*p == '.')
+			for(++p; *p >= '0' && *p <= '9'; ++p)
+				;
+		if(!*p || !strchr("diouxX", *p) || ++conv > 1)
+			return 0;
+	}
+	return 1;
+}
+
 static int
 valid_choices(const struct gray_job *j)
 {
@@ -272,6 +298,8 @@ valid_choices(const struct gray_job *j)
 	if(strcmp(j->term, "eps") && strcmp(j->term, "rplus"))
 		return 0;
 	if(strcmp(j->plan, "measure") && strcmp(j->plan, "estimate"))
+		return 0;
+	if(!valid_pattern(j->outfile) || !valid_pattern(j->rayfile))
 		return 0;
 	return 1;
 }
@@ -522,6 +550,10 @@ init(gray_lux_job *ego)
 	int st;
 	printf("GRay2:init: spacetime:st: %s, initcond:ic: %s\n", EGO->spacetime, EGO->initcond);
 	gray_job_desc(ego, &d);
+	if(EGO->ctx) { /* a second init starts over */
+		gray_destroy(EGO->ctx);
+		EGO->ctx = NULL;
+	}
 	EGO->ctx = gray_create((int)EGO->i_device, 0, &st);
 	if(!EGO->ctx)
 		return st;

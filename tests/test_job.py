@@ -106,10 +106,15 @@ def test_conf_rejects_without_side_effects(job):
     assert job.conf("no_equals_sign") == UNKNOWN
     assert job.conf("a=0.3") == 0
     for bad in ["a=abc", "a=", "N=-1", "W=1x", "st=Minkowski", "ic=pinhole", "scm=RK45",
-                "p=16", "nu=1,-2", "nu=1,2,3,4,5,6,7,8,9", "flow=disk"]:
+                "p=16", "nu=1,-2", "nu=1,2,3,4,5,6,7,8,9", "flow=disk",
+                "out=%s.raw", "out=%d_%d.raw", "out=x%", "out=%ld.raw", "out=%n",
+                "ray=%f.h5"]:
         assert job.conf(bad) == api.EINVAL, bad
     assert job.get("a_spin") == "0.29999999999999999"
     assert job.get("spacetime") == "Kerr"
+    # a dump-name pattern with one integer conversion (or none) is accepted
+    for good in ["out=run%%_%06d.raw", "out=%.4x", "out=final.raw", "out="]:
+        assert job.conf(good) == 0, good
 
 
 def test_raw_dump_format(job, tmp_path):
