@@ -52,8 +52,7 @@ MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 METRIC = "ray-steps/s"
 
 # DRAM bytes (read + write) of one full-size launch of the dominant kernel,
-# from one-pass ncu captures (profiles/mixed_kernel_torus_rt.md,
-# profiles/dyst_mixed_kernel_numerical_128.md).
+# from one-pass ncu captures (dram__bytes_read.sum + dram__bytes_write.sum).
 TRAFFIC = {"torus_rt_1024": 145832704 + 116188928,
            "numerical_128": 500394240 + 17862656}
 # Host-to-device bytes of one render through the C ABI: the render's table

@@ -92,6 +92,9 @@ check_desc(const gray_render_desc *d)
 		return GRAY_EINVAL;
 	if(d->n_sub > (uint64_t)INT32_MAX)
 		return GRAY_EINVAL;
+	/* the persistent kernels count dump intervals in 32-bit integers */
+	if(d->n_dump > (uint64_t)INT32_MAX)
+		return GRAY_EINVAL;
 	if(d->n_freq < 0 || d->n_freq > GRAY_MAX_FREQ)
 		return GRAY_EINVAL;
 	if(d->flow != GRAY_FLOW_NONE && d->flow != GRAY_FLOW_TORUS &&

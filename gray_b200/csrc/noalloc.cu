@@ -71,11 +71,7 @@ gray_run_mixed_noalloc(int device, const gray_render_desc *descs, int n_renders,
 		return GRAY_EINVAL;
 	if(n_renders < 1 || n_renders > GRAY_NOALLOC_MAX_RENDERS)
 		return GRAY_EINVAL; /* beyond the static scratch: at most GRAY_NOALLOC_MAX_RENDERS */
-	if(cudaGetDeviceCount(&n_dev) != cudaSuccess || device < 0 || device >= n_dev ||
-	   device >= MAX_DEVICES) {
-		cudaGetLastError();
-		return GRAY_ENODEV;
-	}
+	/* arguments first, so a bad call is refused before any device is touched */
 	unsigned long long total = 0;
 	for(int i = 0; i < n_renders; ++i) {
 		const gray_render_desc &d = descs[i];
@@ -89,6 +85,11 @@ gray_run_mixed_noalloc(int device, const gray_render_desc *descs, int n_renders,
 	}
 	if(total > (1ull << 31))
 		return GRAY_EINVAL; /* the ray queue is a 32-bit counter */
+	if(cudaGetDeviceCount(&n_dev) != cudaSuccess || device < 0 || device >= n_dev ||
+	   device >= MAX_DEVICES) {
+		cudaGetLastError();
+		return GRAY_ENODEV;
+	}
 
 	int prev = 0;
 	cudaGetDevice(&prev);

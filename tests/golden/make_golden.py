@@ -19,7 +19,7 @@ generates (gray_b200/csrc/make_logk2.py) holds the same numbers as the
 table of sim-org/rt.cl:51-67.
 
 Run from the repository root:
-    python tests/golden/make_golden.py [path/to/reference/tools]
+    python tests/golden/make_golden.py <path/to/reference>/tools
 The fixtures are committed; the tests never need the reference at run time.
 """
 import json
@@ -78,7 +78,9 @@ def rk4(bk, a, s, h):
 
 
 def main():
-    tools = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/tools"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference>/tools  (the reference's tools directory)")
+    tools = sys.argv[1]
     bk = load_tool(tools)
     rng = np.random.default_rng(20261203)
 

@@ -88,3 +88,17 @@ def test_missing_library_fails_loudly(tmp_path):
     p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
     assert p.returncode == 0, p.stderr
     assert "raised:" in p.stdout and "not built" in p.stdout
+
+
+def test_dump_count_beyond_int32_is_refused_before_any_device_call():
+    """The persistent kernels count dump intervals in 32-bit integers, so
+    every entry point refuses n_dump >= 2^31.  The allocation-free entry
+    point validates its descriptors before it looks for a device, so this
+    runs without a GPU."""
+    from gray_b200 import configs
+    L = api.lib()
+    cfg = dict(configs.scaled(configs.TORUS_RT_1024, 8), precision=api.PREC_MIXED)
+    ptrs = (ctypes.c_void_p * 1)(ctypes.c_void_p(16))  # never dereferenced
+    for n_dump, want in ((2 ** 31, api.EINVAL), (2 ** 32 + 4, api.EINVAL)):
+        d = (api.RenderDesc * 1)(api.make_desc(dict(cfg, n_dump=n_dump)))
+        assert L.gray_run_mixed_noalloc(0, d, 1, ptrs, ptrs, None, None) == want

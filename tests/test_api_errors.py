@@ -83,3 +83,16 @@ def test_out_of_order_unknown_and_size_errors(ctx):
     finally:
         r.close()
     assert np.array_equal(data, run(ctx, SMALL))
+
+
+def test_dump_count_beyond_int32_is_refused(ctx):
+    """n_dump >= 2^31 would overflow the kernels' 32-bit dump counters: every
+    create path refuses it with GRAY_EINVAL instead of running the wrong
+    number of intervals."""
+    for prec in (api.PREC_FP64, api.PREC_MIXED):
+        for n_dump in (2 ** 31, 2 ** 32 + 4):
+            with pytest.raises(api.GrayError) as e:
+                ctx.render(dict(SMALL, precision=prec, n_dump=n_dump))
+            assert e.value.status == api.EINVAL
+    ok = ctx.render(dict(SMALL, n_dump=2 ** 31 - 1))  # the largest count is accepted
+    ok.close()
