@@ -14,7 +14,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libgray_cuda.so")
 MAX_FREQ = 8
-ABI_VERSION = 2  # GRAY_ABI_VERSION of include/gray_cuda.h
+ABI_VERSION = 3  # GRAY_ABI_VERSION of include/gray_cuda.h
 
 OK, EINVAL, ENOMEM, ECUDA, ENODEV, EBUDGET, ETIMEOUT, ENOTFOUND, ESTATE, ESIZE, ESOURCE = (
     0, -1, -2, -3, -4, -5, -6, -7, -8, -9, -10)
@@ -71,6 +71,7 @@ class RenderDesc(ctypes.Structure):
         ("spacetime", ctypes.c_int32), ("precision", ctypes.c_int32),
         ("m_adm", ctypes.c_double), ("flow_te", ctypes.c_double),
         ("flow_b", ctypes.c_double),
+        ("row_begin", ctypes.c_uint64), ("n_rows", ctypes.c_uint64),
     ]
 
 
@@ -127,7 +128,7 @@ DEFAULTS = dict(m_bh=4e6, a_spin=0.0, w_img=64.0, h_img=64.0, r_obs=1024.0,
                 dt_dump=-32.0, n_sub=1024, n_dump=64, term=TERM_EPS, nu=(),
                 flow=None, torus_n0=1.0, torus_kappa=1.0, torus_hr=0.3,
                 spacetime=ST_KERR, precision=PREC_FP64, m_adm=4.3e6,
-                flow_te=1e12, flow_b=0.0)
+                flow_te=1e12, flow_b=0.0, row_begin=0, n_rows=0)
 
 
 def make_desc(cfg):
@@ -138,7 +139,8 @@ def make_desc(cfg):
               "t_init", "dt_dump", "torus_n0", "torus_kappa", "torus_hr",
               "m_adm", "flow_te", "flow_b"):
         setattr(d, k, float(c[k]))
-    for k in ("n_width", "n_height", "n_sub", "n_dump", "term", "spacetime", "precision"):
+    for k in ("n_width", "n_height", "n_sub", "n_dump", "term", "spacetime", "precision",
+              "row_begin", "n_rows"):
         setattr(d, k, int(c[k]))
     nu = list(c["nu"])
     if len(nu) > MAX_FREQ:
@@ -253,7 +255,7 @@ class Render:
         _ck(lib().gray_render_create(ctx.h, ctypes.byref(self.desc), ctypes.byref(rid)),
             "gray_render_create")
         self.id = rid.value
-        self.n_rays = self.desc.n_width * self.desc.n_height
+        self.n_rays = self.desc.n_width * (self.desc.n_rows or self.desc.n_height)
         self.n_data = 8 + 2 * self.desc.n_freq
 
     def icond(self):

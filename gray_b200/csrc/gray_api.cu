@@ -88,7 +88,10 @@ check_desc(const gray_render_desc *d)
 		return GRAY_EINVAL;
 	if(d->n_width > (1u << 20) || d->n_height > (1u << 20))
 		return GRAY_EINVAL;
-	if((uint64_t)d->n_width * d->n_height > (1ull << 31))
+	if(d->n_rows == 0 ? d->row_begin != 0
+	                  : d->row_begin >= d->n_height || d->n_rows > d->n_height - d->row_begin)
+		return GRAY_EINVAL;
+	if((uint64_t)d->n_width * (d->n_rows ? d->n_rows : d->n_height) > (1ull << 31))
 		return GRAY_EINVAL;
 	if(d->n_sub > (uint64_t)INT32_MAX)
 		return GRAY_EINVAL;
@@ -146,7 +149,8 @@ make_params(const gray_render_desc *d, RenderParams *p)
 	p->r_obs = d->r_obs;
 	p->w_rays = (long long)d->n_width;
 	p->h_rays = (long long)d->n_height;
-	p->n_rays = p->w_rays * p->h_rays;
+	p->row0 = (long long)d->row_begin;
+	p->n_rays = p->w_rays * (long long)(d->n_rows ? d->n_rows : d->n_height);
 	p->spacetime = d->spacetime;
 	p->flow = d->n_freq > 0 ? d->flow : GRAY_FLOW_NONE;
 	p->n_freq = d->n_freq;

@@ -38,6 +38,7 @@ struct RenderParams {
 	double ci, si, cj, sj;   /* camera angle cosines and sines           */
 	double w_img, h_img, r_obs;
 	long long w_rays, h_rays, n_rays;
+	long long row0;          /* first camera row of the render's rays    */
 	int    n_freq, flow, n_data, spacetime;
 	double torus_n0, torus_kappa, torus_hr;
 	double nupow[GRAY_MAX_FREQ];   /* nu_i^-0.7 */

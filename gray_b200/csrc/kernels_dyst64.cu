@@ -27,7 +27,7 @@ dyst_icond_kernel(const RenderParams p, const GridParams g, double *__restrict__
 	if(r >= p.n_rays)
 		return;
 	const long long gi = r % p.w_rays;
-	const long long gj = r / p.w_rays;
+	const long long gj = p.row0 + r / p.w_rays;
 	double alpha = (((double)gi + 0.5) / (double)p.w_rays - 0.5) * p.w_img;
 	double beta  = (((double)gj + 0.5) / (double)p.h_rays - 0.5) * p.h_img;
 	double R0 = fma(p.r_obs, p.si, -(beta * p.ci));

@@ -294,7 +294,7 @@ icond64_kernel(const RenderParams p, double *__restrict__ data,
 	if(g >= p.n_rays)
 		return;
 	const long long gi = g % p.w_rays;
-	const long long gj = g / p.w_rays;
+	const long long gj = p.row0 + g / p.w_rays;
 	double alpha = (((double)gi + 0.5) / (double)p.w_rays - 0.5) * p.w_img;
 	double beta  = (((double)gj + 0.5) / (double)p.h_rays - 0.5) * p.h_img;
 

@@ -7,9 +7,15 @@
  *    lanes whose ray terminated (horizon capture, or its dump window done)
  *    and refills exactly those lanes, so captured rays do not idle SIMD
  *    lanes while their neighbours keep integrating;
- *  - the RHS (KS.cl:263-378), RK4 stages (RK4.cl:37-47) and transfer
- *    (rt.cl:185-198 form with the analytic torus) run in FP32 with the
- *    approximate rcp/rsqrt/ex2/lg2 instructions in place of IEEE divide and
+ *  - the geodesic equation (KS.cl:263-378) is integrated in Hamiltonian
+ *    form, on the event x^mu and the covariant momentum k_mu: k_t is
+ *    conserved and the force needs no gradient of l, so a step costs about
+ *    a third fewer operations than the second-order form in u^mu; u^mu
+ *    (the state in HBM) is converted to k_mu in FP64 when a ray is loaded
+ *    and back when it is stored;
+ *  - the RHS, RK4 stages (RK4.cl:37-47) and transfer (rt.cl:185-198 form
+ *    with the analytic torus) run in FP32 with the approximate
+ *    rcp/rsqrt/ex2/lg2 instructions in place of IEEE divide and
  *    square-root sequences; with two rays per thread the whole step runs in
  *    sm_100 packed f32x2 arithmetic (one FFMA2/FMUL2/FADD2 issue slot serves
  *    both rays), and with one ray per thread the RK4 stage sums, stage
@@ -156,27 +162,57 @@ template <> struct Lanes<F2> { static constexpr int N = 2; };
 
 /* ------------------------------------------------ per-ray render constants */
 
-template <typename V, int NF>
-struct RC {
-	V a, aa, risco, kappa, n0t, ihr2;
-	V lgnupow[NF > 0 ? NF : 1], nuinv2[NF > 0 ? NF : 1];
+/* Register layout of a ray in the mixed kernel: the event x^mu, the spatial
+ * covariant momentum k_i, then I_nu and the optical depth of the first
+ * frequency.  k_t is conserved (the metric does not depend on t) and lives
+ * in RC.  For the torus every frequency's absorption is the same function
+ * of the ray times nu_i^-2 (alpha_nu = kappa n nu^-2 at the fluid-frame
+ * frequency, dtau_i = -alpha shift), so tau_i - tau_i(0) = (nu_0/nu_i)^2
+ * (tau_0 - tau_0(0)) holds exactly and only tau_0 is integrated. */
+template <int NF>
+struct Layout {
+	static constexpr int NI = 7 + (NF > 0 ? NF + 1 : 0); /* integrated reals     */
+	static constexpr int I0 = 7;                        /* first I_nu           */
+	static constexpr int TAU = 7 + NF;                  /* tau of frequency 0   */
+	static constexpr int ND = 8 + 2 * NF;               /* reals in HBM per ray */
 };
 
 template <typename V, int NF>
+struct RC {
+	V a, aa, risco, n0t, ihr2, kap0, kt;
+	/* log2(nu_i^-0.7) plus the frequency's optical-depth offset, and the
+	 * factor turning tau_0 into -log2(e) tau_i */
+	V lgnu[NF > 0 ? NF : 1], tcoef[NF > 0 ? NF : 1];
+};
+
+/* (nu_0/nu_i)^2: tau_i - tau_i(0) = (nu_0/nu_i)^2 (tau_0 - tau_0(0)); the
+ * offset tau_i(0) - (nu_0/nu_i)^2 tau_0(0), zero for rays that start at the
+ * camera, is folded into the frequency's constant. */
+__device__ __forceinline__ double
+tau_ratio(const MixedRender &c, int i)
+{
+	const double q = c.nu_hz[0] / c.nu_hz[i];
+	return q * q;
+}
+
+template <typename V, int NF>
 __device__ __forceinline__ void
-load_rc(RC<V, NF> &rc, int k, const MixedRender &c)
+load_rc(RC<V, NF> &rc, int k, const MixedRender &c, double kt, const double *tau0)
 {
 	setl(rc.a, k, c.a);
 	setl(rc.aa, k, c.aa);
 	setl(rc.risco, k, c.risco);
-	setl(rc.kappa, k, c.kappa);
 	/* the density scale, zero without the torus flow */
 	setl(rc.n0t, k, c.flow == GRAY_FLOW_TORUS ? c.n0_rp15 : 0.0f);
 	setl(rc.ihr2, k, c.ihr2_log2e);
+	setl(rc.kap0, k, NF > 0 ? c.kappa * c.nuinv2[0] : 0.0f);
+	setl(rc.kt, k, (float)kt);
 #pragma unroll
 	for(int i = 0; i < NF; ++i) {
-		setl(rc.lgnupow[i], k, log2f(c.nupow[i])); /* nu_i^-0.7 as a power of 2 */
-		setl(rc.nuinv2[i], k, c.nuinv2[i]);
+		const double q = tau_ratio(c, i);
+		const double off = tau0[i] - q * tau0[0];
+		setl(rc.lgnu[i], k, log2f(c.nupow[i]) - (float)(1.4426950408889634 * off));
+		setl(rc.tcoef[i], k, (float)(-1.4426950408889634 * q));
 	}
 }
 
@@ -184,154 +220,108 @@ load_rc(RC<V, NF> &rc, int k, const MixedRender &c)
 
 template <typename V>
 struct Aux {
-	V r, ir, f, lx, ly, lz, flu, iss, R2;
+	V r, ir, f, iss, R2;
 };
 
-/* KS.cl:263-378 in FP32: the Chan et al. grouping, with the five divides
- * and two square roots folded into 2 rsqrt + 2 rcp. */
+/* The geodesic equation of KS.cl:263-378 in Hamiltonian form.  With
+ * g^{mu nu} = eta^{mu nu} - f l^mu l^nu (l^mu = (-1, l_x, l_y, l_z)) and
+ * L = l^mu k_mu, Hamilton's equations for H = g^{mu nu} k_mu k_nu / 2 are
+ *   dx^mu/dl = eta^{mu nu} k_nu - f L l^mu
+ *   dk_i/dl  = f L d_i L + L^2 d_i f / 2,   dk_t/dl = 0,
+ * the same geodesics as the reference's second-order form in u^mu (the
+ * state is mapped u <-> k with down() in FP64 when a ray is loaded and
+ * stored).  f, l and r share the reference's radius root and gradient; the
+ * r-dependence of L and f enters through d_i r once:
+ *   d_i L = dL/dr d_i r + (explicit part),  dL/dr = iss (x k_x + y k_y
+ *   - 2 r (l_x k_x + l_y k_y)) - l_z k_z / r,
+ * so dk_i = G d_i r + f L (explicit d_i L) [+ L^2 df/dz|_r / 2 for z] with
+ * G = f L dL/dr + L^2 df/dr / 2, and no gradient of l is formed. */
 template <typename V, int NF>
 __device__ __forceinline__ void
-ks_rhs(const RC<V, NF> &c, const V *s, V *ds, Aux<V> &aux)
+ks_ham(const RC<V, NF> &c, const V *s, V *ds, Aux<V> &aux)
 {
-	const V a = c.a, aa = c.aa;
+	const V a = c.a, aa = c.aa, kt = c.kt;
 	const V x = s[1], y = s[2], z = s[3];
-	const V ut = s[4], ux = s[5], uy = s[6], uz = s[7];
-	const V half = bc<V>(0.5f), one = bc<V>(1.0f), two = bc<V>(2.0f);
+	const V kx = s[4], ky = s[5], kz = s[6];
+	const V half = bc<V>(0.5f), two = bc<V>(2.0f);
 
-	V f, dx_f, dy_f, dz_f;
-	V lx, dx_lx, dy_lx, dz_lx;
-	V ly, dx_ly, dy_ly, dz_ly;
-	V lz, dx_lz, dy_lz, dz_lz;
-	V dx_r, dy_r, dz_r, r, ir, iss, tmp, R2;
-	{
-		V zz  = z * z;
-		V azz = aa * zz;
-		R2       = fmav(x, x, y * y); /* also the torus's cylindrical radius */
-		V kk  = half * ((R2 + zz) - aa);
-		V d2  = fmav(kk, kk, azz);
-		V idd = rsqv(d2);
-		V rr  = fmav(d2, idd, kk);    /* sqrt(d2) + kk */
-		ir  = rsqv(rr);
-		r   = rr * ir;
-		V ss = rr + aa;
-		iss  = rcpv(ss);
-		tmp  = half * (ir * idd);
-		dz_r = (tmp * ss) * z;
-		tmp  = tmp * rr;
-		dy_r = tmp * y;
-		dx_r = tmp * x;
-		tmp  = (two * rr) * rcpv(fmav(rr, rr, azz));
-		V tmp2 = fmav(-(two * rr), tmp, bc<V>(3.0f));
-		f    = tmp * r;
-		V tt2 = tmp * tmp2;
-		dx_f = tt2 * dx_r;
-		dy_f = tt2 * dy_r;
-		dz_f = fmav(tt2, dz_r, -((tmp * tmp) * (aa * (z * ir))));
-	}
-	{
-		V m2r  = -(two * r);
-		V issr = iss * r;
-		V issa = iss * a;
+	V zz  = z * z;
+	V azz = aa * zz;
+	V R2  = fmav(x, x, y * y);       /* also the torus's cylindrical radius */
+	V kk  = half * ((R2 + zz) - aa);
+	V d2  = fmav(kk, kk, azz);
+	V idd = rsqv(d2);
+	V rr  = fmav(d2, idd, kk);       /* r^2 = sqrt(d2) + kk */
+	V ir  = rsqv(rr);
+	V r   = rr * ir;
+	V ss  = rr + aa;
+	V iss = rcpv(ss);
+	V hrd = half * (ir * idd);       /* d_x r = hrd r^2 x, d_z r = hrd ss z */
+	V t   = (two * rr) * rcpv(fmav(rr, rr, azz)); /* f / r */
+	V f   = t * r;
+	V tt2 = t * fmav(-(two * rr), t, bc<V>(3.0f)); /* df/dr */
+	V fz  = -((t * t) * (aa * (z * ir)));          /* df/dz at fixed r */
 
-		lx    = iss * fmav(x, r, y * a);
-		tmp   = iss * fmav(m2r, lx, x);
-		dx_lx = fmav(tmp, dx_r, issr);
-		dy_lx = fmav(tmp, dy_r, issa);
-		dz_lx = tmp * dz_r;
+	V lx = iss * fmav(x, r, y * a);
+	V ly = iss * fmav(y, r, -(x * a));
+	V lz = z * ir;
+	V P  = fmav(ly, ky, lx * kx);
+	V L  = fmav(lz, kz, P - kt);
+	V Q  = fmav(y, ky, x * kx);
+	V dLdr = fmav(iss, fmav(-(two * r), P, Q), -((lz * ir) * kz));
+	V fL  = f * L;
+	V hLL = (half * L) * L;
+	V G   = fmav(fL, dLdr, hLL * tt2);
+	V Gxy = G * (hrd * rr);
+	V Gz  = G * (hrd * ss);
+	V fLi = fL * iss;
 
-		ly    = iss * fmav(y, r, -(x * a));
-		tmp   = iss * fmav(m2r, ly, y);
-		dx_ly = fmav(tmp, dx_r, -issa);
-		dy_ly = fmav(tmp, dy_r, issr);
-		dz_ly = tmp * dz_r;
+	ds[0] = fL - kt;
+	ds[1] = fmav(-fL, lx, kx);
+	ds[2] = fmav(-fL, ly, ky);
+	ds[3] = fmav(-fL, lz, kz);
+	ds[4] = fmav(Gxy, x, fLi * fmav(r, kx, -(a * ky)));
+	ds[5] = fmav(Gxy, y, fLi * fmav(r, ky, a * kx));
+	ds[6] = fmav(Gz, z, fmav(fL * ir, kz, hLL * fz));
 
-		lz    = z * ir;
-		tmp   = -(lz * ir);
-		dx_lz = tmp * dx_r;
-		dy_lz = tmp * dy_r;
-		dz_lz = fmav(tmp, dz_r, ir);
-	}
-	V lu  = fmav(lz, uz, fmav(ly, uy, fmav(lx, ux, ut)));
-	V flu = f * lu;
-	/* KS.cl:340-363 form the covector derivatives D_a = d_a(f l.u l) (a =
-	 * x, y, z) component by component and contract them twice.  With
-	 * D_a^0 = d_a f (l.u) + f (d_a l . u) and D_a^i = D_a^0 l^i + f l.u d_a l^i
-	 * the two contractions are, exactly,
-	 *   hD_a u = (D_a^0 l.u + f l.u (d_a l . u)) / 2
-	 *   uD^i   = uD^0 l^i + f l.u (u . grad) l^i,
-	 * which skips the nine D_a^i (same mathematics, fewer operations). */
-	V Lx = fmav(dx_lz, uz, fmav(dx_ly, uy, dx_lx * ux)); /* d_x l . u */
-	V Ly = fmav(dy_lz, uz, fmav(dy_ly, uy, dy_lx * ux));
-	V Lz = fmav(dz_lz, uz, fmav(dz_ly, uy, dz_lx * ux));
-	V Dx0 = fmav(dx_f, lu, f * Lx);
-	V Dy0 = fmav(dy_f, lu, f * Ly);
-	V Dz0 = fmav(dz_f, lu, f * Lz);
-	V hlu = half * lu, hflu = half * flu;
-	V hDxu = fmav(Dx0, hlu, hflu * Lx);
-	V hDyu = fmav(Dy0, hlu, hflu * Ly);
-	V hDzu = fmav(Dz0, hlu, hflu * Lz);
-	V uD0 = fmav(uz, Dz0, fmav(uy, Dy0, ux * Dx0));
-	V Mx  = fmav(uz, dz_lx, fmav(uy, dy_lx, ux * dx_lx)); /* (u . grad) l */
-	V My  = fmav(uz, dz_ly, fmav(uy, dy_ly, ux * dx_ly));
-	V Mz  = fmav(uz, dz_lz, fmav(uy, dy_lz, ux * dx_lz));
-	V uD1 = fmav(uD0, lx, flu * Mx);
-	V uD2 = fmav(uD0, ly, flu * My);
-	V uD3 = fmav(uD0, lz, flu * Mz);
-
-	tmp = f * fmav(lz, uD3 - hDzu, fmav(ly, uD2 - hDyu, fmav(lx, uD1 - hDxu, -uD0)));
-
-	ds[0] = ut;
-	ds[1] = ux;
-	ds[2] = uy;
-	ds[3] = uz;
-	ds[4] = uD0 - tmp;
-	ds[5] = fmav(lx, tmp, hDxu - uD1);
-	ds[6] = fmav(ly, tmp, hDyu - uD2);
-	ds[7] = fmav(lz, tmp, hDzu - uD3);
-
-	aux.r = r; aux.ir = ir; aux.f = f; aux.lx = lx; aux.ly = ly; aux.lz = lz; aux.R2 = R2;
-	aux.flu = flu; aux.iss = iss;
-	(void)one;
+	aux.r = r; aux.ir = ir; aux.f = f; aux.iss = iss; aux.R2 = R2;
 }
 
-/* Torus flow + transfer (same model as the FP64 kernel), branch-free: the
- * emission is masked to zero outside r_isco, where the Keplerian flow is not
- * timelike, or where the shift is not positive. */
+/* Torus flow + transfer (the FP64 kernel's model), branch-free: the
+ * emission is masked to zero outside r_isco, where the Keplerian flow is
+ * not timelike, or where the shift is not positive.  The shift is -k_mu
+ * u^mu_fluid with k_mu straight from the state.  Every factor is folded into
+ * one power of 2 per output:
+ *   dtau_0 = -kappa nu_0^-2 n / shift
+ *   dI_i   = -n nu_i^-0.7 shift^-2.7 e^-tau_i
+ * with n = n0 (r_+/r)^1.5 exp(-z^2 / (2 (h r)^2)). */
 template <typename V, int NF>
 __device__ __forceinline__ void
 torus_rt(const RC<V, NF> &c, const V *s, const Aux<V> &x, V *ds)
 {
+	typedef Layout<NF> Y;
 	typedef typename MaskOf<V>::T M;
 	const V one = bc<V>(1.0f), zero = bc<V>(0.0f);
 	const V q1 = s[1], q2 = s[2], q3 = s[3];
-	V kt  = x.flu - s[4];
-	V kx  = fmav(x.flu, x.lx, s[5]);
-	V ky  = fmav(x.flu, x.ly, s[6]);
-	const V R2 = x.R2;
+	const V kx = s[4], ky = s[5];
 	V irs = rsqv(x.r);                 /* r^-1/2 */
 	V sr  = x.r * irs;                 /* r^1/2  */
 	V Om  = rcpv(fmav(x.r, sr, c.a));
-	V vv  = fmav(Om * Om, R2, -one);
-	V lv  = fmav(-((c.a * Om) * R2), x.iss, one);
+	V vv  = fmav(Om * Om, x.R2, -one);
+	V lv  = fmav(-((c.a * Om) * x.R2), x.iss, one);
 	V D   = -fmav(x.f * lv, lv, vv);
 	M ok  = andv(gtv(x.r, c.risco), gtv(D, zero));
 	V utf = rsqv(selv(ok, D, one));
-	V shift = -(utf * fmav(Om, fmav(q1, ky, -(q2 * kx)), kt));
+	V shift = -(utf * fmav(Om, fmav(q1, ky, -(q2 * kx)), c.kt));
 	ok = andv(ok, gtv(shift, zero));
-	V sh = selv(ok, shift, one);
-	/* n0 (r_+/r)^1.5 exp(-z^2 / (2 (h r)^2)) */
-	V e = ex2v(-((q3 * q3) * ((x.ir * x.ir) * c.ihr2)));
-	V n = selv(ok, c.n0t * ((x.ir * irs) * e), zero);
-	/* -j(nu) / shift^2 = -n nu_i^-0.7 shift^-2.7: one power of the shift
-	 * for all frequencies, nu_i^-0.7 e^-tau_i as one power of 2 each */
-	V mjis2 = -(n * ex2v(bc<V>(-2.7f) * lg2v(sh)));
-	V mtfac = -((c.kappa * n) * rcpv(sh));
-	const V mlog2e = bc<V>(-1.4426950408889634f);
+	V lsh = lg2v(selv(ok, shift, one));
+	V gz  = -((q3 * q3) * ((x.ir * x.ir) * c.ihr2));  /* log2 of the Gaussian */
+	V A   = selv(ok, -(c.n0t * (x.ir * irs)), zero);  /* -n0 (r_+/r)^1.5 */
+	ds[Y::TAU] = (A * c.kap0) * ex2v(gz - lsh);
+	V g27 = fmav(bc<V>(-2.7f), lsh, gz);
 #pragma unroll
-	for(int i = 0; i < NF; ++i) {
-		ds[8 + i]      = mjis2 * ex2v(fmav(s[8 + NF + i], mlog2e, c.lgnupow[i]));
-		ds[8 + NF + i] = mtfac * c.nuinv2[i];
-	}
+	for(int i = 0; i < NF; ++i)
+		ds[Y::I0 + i] = A * ex2v(fmav(s[Y::TAU], c.tcoef[i], g27 + c.lgnu[i]));
 }
 
 template <typename V, int NF>
@@ -339,7 +329,7 @@ __device__ __forceinline__ void
 rhs(const RC<V, NF> &c, const V *s, V *ds)
 {
 	Aux<V> aux;
-	ks_rhs<V, NF>(c, s, ds, aux);
+	ks_ham<V, NF>(c, s, ds, aux);
 	if(NF > 0)
 		torus_rt<V, NF>(c, s, aux, ds);
 }
@@ -355,27 +345,55 @@ getrr_d(double aa, double x, double y, double z)
 	return sqrt(fma(kk, kk, aa * zz)) + kk;
 }
 
-/* KS.cl:164-168 null constraint from the final state */
+/* f and l_mu = (1, l_x, l_y, l_z) at an event (KS.cl:282-333) */
+__device__ __forceinline__ void
+fl_d(double a, const double *q, double *f, double *l)
+{
+	double aa = a * a;
+	double zz = q[3] * q[3];
+	double kk = 0.5 * (fma(q[1], q[1], fma(q[2], q[2], zz)) - aa);
+	double rr = sqrt(fma(kk, kk, aa * zz)) + kk;
+	double r  = sqrt(rr);
+	*f = 2.0 * rr * r / fma(rr, rr, aa * zz);
+	double iss = 1.0 / (rr + aa);
+	l[0] = iss * fma(q[1], r, q[2] * a);
+	l[1] = iss * fma(q[2], r, -(q[1] * a));
+	l[2] = q[3] / r;
+}
+
+/* KS.cl:91-114 down(): k_mu = g_mu_nu u^nu = eta u + f (l.u) l */
+__device__ __forceinline__ void
+down_d(double a, const double *q, const double *u, double *k)
+{
+	double f, l[3];
+	fl_d(a, q, &f, l);
+	double flu = f * fma(l[2], u[3], fma(l[1], u[2], fma(l[0], u[1], u[0])));
+	k[0] = flu - u[0];
+	k[1] = fma(flu, l[0], u[1]);
+	k[2] = fma(flu, l[1], u[2]);
+	k[3] = fma(flu, l[2], u[3]);
+}
+
+/* its inverse: u^mu = g^{mu nu} k_nu = eta k - f (l^nu k_nu) l^mu */
+__device__ __forceinline__ void
+up_d(double a, const double *q, const double *k, double *u)
+{
+	double f, l[3];
+	fl_d(a, q, &f, l);
+	double fL = f * fma(l[2], k[3], fma(l[1], k[2], fma(l[0], k[1], -k[0])));
+	u[0] = fL - k[0];
+	u[1] = fma(-fL, l[0], k[1]);
+	u[2] = fma(-fL, l[1], k[2]);
+	u[3] = fma(-fL, l[2], k[3]);
+}
+
+/* KS.cl:164-168 null constraint g(u,u) from the final state */
 __device__ __forceinline__ double
 getuu_d(double a, const double *s)
 {
-	double aa = a * a;
-	double zz = s[3] * s[3];
-	double kk = 0.5 * (fma(s[1], s[1], fma(s[2], s[2], zz)) - aa);
-	double rr = sqrt(fma(kk, kk, aa * zz)) + kk;
-	double r  = sqrt(rr);
-	double f  = 2.0 * rr * r / fma(rr, rr, aa * zz);
-	double iss = 1.0 / (rr + aa);
-	double lx = iss * fma(s[1], r, s[2] * a);
-	double ly = iss * fma(s[2], r, -(s[1] * a));
-	double lz = s[3] / r;
-	double lu = fma(lz, s[7], fma(ly, s[6], fma(lx, s[5], s[4])));
-	double flu = f * lu;
-	double k0 = flu - s[4];
-	double k1 = fma(flu, lx, s[5]);
-	double k2 = fma(flu, ly, s[6]);
-	double k3 = fma(flu, lz, s[7]);
-	return fma(k3, s[7], fma(k2, s[6], fma(k1, s[5], k0 * s[4])));
+	double k[4];
+	down_d(a, s, s + 4, k);
+	return fma(k[3], s[7], fma(k[2], s[6], fma(k[1], s[5], k[0] * s[4])));
 }
 
 /* ------------------------------------------------------ slot bookkeeping */
@@ -408,19 +426,60 @@ start_dump(Slot &S)
 	S.h      = 0;
 }
 
-template <typename V, int ND>
+/* Final state to HBM in the reference's layout: x^mu, u^mu (from k_mu in
+ * FP64), I_nu, tau_nu (tau_i rebuilt from tau_0) and g(u,u).  The ray's
+ * state as it was loaded is still in HBM: k_t is recomputed from it (the
+ * same FP64 value the load computed) and the initial tau_i are read from it
+ * before they are overwritten.  Called once per ray and dump window, so it
+ * is kept out of line: its FP64 temporaries do not add to the register
+ * count of the stepping loop. */
+__device__ __noinline__ void
+store_ray(const MixedRender &c, long long ray, int nf, const float *hi, const float *lo)
+{
+	const long long nr = c.n_rays;
+	double q[4], k[4], u[4];
+	{
+		double s0[8];
+		for(int i = 0; i < 8; ++i)
+			s0[i] = c.data[i * nr + ray];
+		down_d(c.a_d, s0, s0 + 4, k);
+	}
+	for(int i = 0; i < 4; ++i)
+		q[i] = (double)hi[i] - (double)lo[i];
+	for(int i = 1; i < 4; ++i)
+		k[i] = (double)hi[3 + i] - (double)lo[3 + i];
+	up_d(c.a_d, q, k, u);
+	for(int i = 0; i < 4; ++i) {
+		c.data[i * nr + ray] = q[i];
+		c.data[(4 + i) * nr + ray] = u[i];
+	}
+	if(nf > 0) {
+		const double tau = (double)hi[7 + nf] - (double)lo[7 + nf];
+		const double tau00 = c.data[(8 + nf) * nr + ray];
+		for(int i = 1; i < nf; ++i) {
+			double *p = c.data + (8 + nf + i) * nr + ray;
+			*p = fma(tau_ratio(c, i), tau - tau00, *p);
+		}
+		c.data[(8 + nf) * nr + ray] = tau;
+		for(int i = 0; i < nf; ++i)
+			c.data[(8 + i) * nr + ray] = (double)hi[7 + i] - (double)lo[7 + i];
+	}
+	double s[8] = {q[0], q[1], q[2], q[3], u[0], u[1], u[2], u[3]};
+	c.info[ray] = getuu_d(c.a_d, s);
+}
+
+template <typename V, int NF>
 __device__ __forceinline__ void
 store_slot(const Slot &S, int k, const V *hi, const V *lo)
 {
-	const MixedRender &c = *S.c;
-	const long long nr = c.n_rays;
-	double s[ND];
+	constexpr int NI = Layout<NF>::NI;
+	float h[NI], l[NI];
 #pragma unroll
-	for(int i = 0; i < ND; ++i) {
-		s[i] = (double)getl(hi[i], k) - (double)getl(lo[i], k);
-		c.data[i * nr + S.ray] = s[i];
+	for(int i = 0; i < NI; ++i) {
+		h[i] = getl(hi[i], k);
+		l[i] = getl(lo[i], k);
 	}
-	c.info[S.ray] = getuu_d(c.a_d, s);
+	store_ray(*S.c, S.ray, NF, h, l);
 }
 
 /* Map a global queue index to (render, ray) by binary search over the
@@ -464,17 +523,93 @@ ticks(const Slot &S, int k, const V *hi, const V *lo)
 	return dh < S.n - S.h ? dh : S.n - S.h;
 }
 
+/* One RK4 step (RK4.cl:37-47) of size hs on the NI integrated reals with
+ * the compensated update (value = hi - lo).  With one ray per thread the
+ * stage sums, stage states and update run on pairs of components (2j,
+ * 2j+1) in packed f32x2, one instruction per pair; an odd last component
+ * runs scalar.  The roundings are those of the lane-wise form, except that
+ * a product feeding an add is not contracted into an FMA. */
+template <typename V, int NF>
+__device__ __forceinline__ void
+rk4_packed(const RC<V, NF> &rc, V *hi, V *lo, V hs)
+{
+	constexpr int NI = Layout<NF>::NI;
+	constexpr int NP = NI / 2;
+	constexpr bool TAIL = NI & 1;
+	const V hh = bc<V>(0.5f) * hs;
+	V kk[NI], t[NI];
+	float2 H[NP], S2[NP];
+	float tS = 0.0f;
+	const float2 hh2 = make_float2(hh, hh), hs2 = make_float2(hs, hs);
+	const float2 two2 = make_float2(2.0f, 2.0f);
+#pragma unroll
+	for(int j = 0; j < NP; ++j)
+		H[j] = make_float2(hi[2 * j], hi[2 * j + 1]);
+	rhs<V, NF>(rc, hi, kk);
+#pragma unroll
+	for(int j = 0; j < NP; ++j) {
+		S2[j] = make_float2(kk[2 * j], kk[2 * j + 1]);
+		const float2 s = __ffma2_rn(hh2, S2[j], H[j]);
+		t[2 * j] = s.x;
+		t[2 * j + 1] = s.y;
+	}
+	if(TAIL) {
+		tS = kk[NI - 1];
+		t[NI - 1] = fmaf(hh, kk[NI - 1], hi[NI - 1]);
+	}
+#pragma unroll
+	for(int st = 1; st < 3; ++st) {
+		rhs<V, NF>(rc, t, kk);
+		const float2 c2 = st == 1 ? hh2 : hs2;
+#pragma unroll
+		for(int j = 0; j < NP; ++j) {
+			const float2 K = make_float2(kk[2 * j], kk[2 * j + 1]);
+			S2[j] = __ffma2_rn(two2, K, S2[j]);
+			const float2 s = __ffma2_rn(c2, K, H[j]);
+			t[2 * j] = s.x;
+			t[2 * j + 1] = s.y;
+		}
+		if(TAIL) {
+			tS = fmaf(2.0f, kk[NI - 1], tS);
+			t[NI - 1] = fmaf(st == 1 ? hh : hs, kk[NI - 1], hi[NI - 1]);
+		}
+	}
+	rhs<V, NF>(rc, t, kk);
+	const float h6 = hs * (1.0f / 6.0f);
+	const float2 h62 = make_float2(h6, h6);
+#pragma unroll
+	for(int j = 0; j < NP; ++j) {
+		const float2 K   = make_float2(kk[2 * j], kk[2 * j + 1]);
+		const float2 inc = __fmul2_rn(h62, __fadd2_rn(S2[j], K));
+		const float2 yv  = sub2(inc, make_float2(lo[2 * j], lo[2 * j + 1]));
+		const float2 tv  = __fadd2_rn(H[j], yv);
+		const float2 c   = sub2(sub2(tv, H[j]), yv);
+		hi[2 * j] = tv.x;
+		hi[2 * j + 1] = tv.y;
+		lo[2 * j] = c.x;
+		lo[2 * j + 1] = c.y;
+	}
+	if(TAIL) {
+		const float inc = h6 * (tS + kk[NI - 1]);
+		const float yv = inc - lo[NI - 1];
+		const float tv = hi[NI - 1] + yv;
+		lo[NI - 1] = (tv - hi[NI - 1]) - yv;
+		hi[NI - 1] = tv;
+	}
+}
+
 template <int NF, typename V, bool ROLLED>
-__global__ void __launch_bounds__(Lanes<V>::N == 1 ? 256 : 128)
+__global__ void __launch_bounds__(Lanes<V>::N == 1 ? 256 : 128, Lanes<V>::N == 1 ? 2 : 1)
 mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
              unsigned long long *__restrict__ steps)
 {
-	constexpr int ND = 8 + 2 * NF;
+	typedef Layout<NF> Y;
+	constexpr int NI = Y::NI;
 	constexpr int L = Lanes<V>::N;
 	const unsigned FULL = 0xffffffffu;
 	const int lane = threadIdx.x & 31;
 
-	V hi[ND], lo[ND];
+	V hi[NI], lo[NI];
 	RC<V, NF> rc;
 	Slot S[L];
 	bool exhausted = false;
@@ -483,7 +618,7 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 	for(int k = 0; k < L; ++k)
 		S[k].active = false;
 #pragma unroll
-	for(int i = 0; i < ND; ++i) {
+	for(int i = 0; i < NI; ++i) {
 		hi[i] = bc<V>(0.0f);
 		lo[i] = bc<V>(0.0f);
 	}
@@ -522,18 +657,32 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 			s.cdt_scale = c.cdt_scale;
 			s.aa_d = c.aa_d;
 			s.rp_d = c.rp_d;
-			load_rc<V, NF>(rc, k, c);
 			const long long nr = c.n_rays;
+			double s0[8], k0[4], tau0[NF > 0 ? NF : 1];
 #pragma unroll
-			for(int i = 0; i < ND; ++i) {
-				double v = c.data[i * nr + s.ray];
-				float h = (float)v;
-				setl(hi[i], k, h);
-				setl(lo[i], k, (float)((double)h - v));
-			}
+			for(int i = 0; i < 8; ++i)
+				s0[i] = c.data[i * nr + s.ray];
 			if(s.dump >= s.dump_end) { /* empty window: state unchanged */
-				store_slot<V, ND>(s, k, hi, lo);
+				c.info[s.ray] = getuu_d(c.a_d, s0);
 				continue;
+			}
+			down_d(c.a_d, s0, s0 + 4, k0);
+			double v[NI];
+			v[0] = s0[0]; v[1] = s0[1]; v[2] = s0[2]; v[3] = s0[3];
+			v[4] = k0[1]; v[5] = k0[2]; v[6] = k0[3];
+#pragma unroll
+			for(int i = 0; i < NF; ++i) {
+				v[Y::I0 + i] = c.data[(8 + i) * nr + s.ray];
+				tau0[i] = c.data[(8 + NF + i) * nr + s.ray];
+			}
+			if(NF > 0)
+				v[Y::TAU] = tau0[0];
+			load_rc<V, NF>(rc, k, c, k0[0], tau0);
+#pragma unroll
+			for(int i = 0; i < NI; ++i) {
+				float h = (float)v[i];
+				setl(hi[i], k, h);
+				setl(lo[i], k, (float)((double)h - v[i]));
 			}
 			start_dump(s);
 			s.active = true;
@@ -555,7 +704,7 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 				continue;
 			dh[k] = ticks<V>(S[k], k, hi, lo);
 			if(dh[k] == 0) {
-				store_slot<V, ND>(S[k], k, hi, lo);
+				store_slot<V, NF>(S[k], k, hi, lo);
 				S[k].active = false;
 			} else {
 				step = true;
@@ -569,13 +718,13 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 #pragma unroll
 		for(int k = 0; k < L; ++k)
 			setl(hs, k, (float)dh[k] * S[k].dtn);
-		const V hh = bc<V>(0.5f) * hs;
 		if constexpr(ROLLED) {
 			/* one RHS body, looped over the stages (less code, same
 			 * arithmetic) */
-			V kk[ND], t[ND], sum[ND];
+			const V hh = bc<V>(0.5f) * hs;
+			V kk[NI], t[NI], sum[NI];
 #pragma unroll
-			for(int i = 0; i < ND; ++i)
+			for(int i = 0; i < NI; ++i)
 				t[i] = hi[i];
 #pragma unroll 1
 			for(int st = 0; st < 4; ++st) {
@@ -583,7 +732,7 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 				const V wg = bc<V>((st == 1 || st == 2) ? 2.0f : 1.0f);
 				const V cg = st < 2 ? hh : hs;
 #pragma unroll
-				for(int i = 0; i < ND; ++i) {
+				for(int i = 0; i < NI; ++i) {
 					if(st < 3)
 						sum[i] = st == 0 ? kk[i] : fmav(wg, kk[i], sum[i]);
 					t[i] = fmav(cg, kk[i], hi[i]);
@@ -591,7 +740,7 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 			}
 			const V h6 = hs * bc<V>(1.0f / 6.0f);
 #pragma unroll
-			for(int i = 0; i < ND; ++i) {
+			for(int i = 0; i < NI; ++i) {
 				V inc = h6 * (sum[i] + kk[i]);
 				V yv = inc - lo[i];
 				V tv = hi[i] + yv;
@@ -599,84 +748,32 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 				hi[i] = tv;
 			}
 		} else if constexpr(L == 1) {
-			/* the same stages with the bookkeeping on component pairs
-			 * (2j, 2j+1; ND is even): each stage sum, stage state and
-			 * compensated update is one packed f32x2 instruction per
-			 * pair.  The operations and roundings are those of the
-			 * lane-wise form below, except that a product feeding an
-			 * add is not contracted into an FMA here */
-			constexpr int NP = ND / 2;
-			V kk[ND], t[ND];
-			float2 H[NP], S2[NP];
-			const float2 hh2 = make_float2(hh, hh), hs2 = make_float2(hs, hs);
-			const float2 two2 = make_float2(2.0f, 2.0f);
-#pragma unroll
-			for(int j = 0; j < NP; ++j)
-				H[j] = make_float2(hi[2 * j], hi[2 * j + 1]);
-			rhs<V, NF>(rc, hi, kk);
-#pragma unroll
-			for(int j = 0; j < NP; ++j) {
-				S2[j] = make_float2(kk[2 * j], kk[2 * j + 1]);
-				const float2 s = __ffma2_rn(hh2, S2[j], H[j]);
-				t[2 * j] = s.x;
-				t[2 * j + 1] = s.y;
-			}
-			rhs<V, NF>(rc, t, kk);
-#pragma unroll
-			for(int j = 0; j < NP; ++j) {
-				const float2 K = make_float2(kk[2 * j], kk[2 * j + 1]);
-				S2[j] = __ffma2_rn(two2, K, S2[j]);
-				const float2 s = __ffma2_rn(hh2, K, H[j]);
-				t[2 * j] = s.x;
-				t[2 * j + 1] = s.y;
-			}
-			rhs<V, NF>(rc, t, kk);
-#pragma unroll
-			for(int j = 0; j < NP; ++j) {
-				const float2 K = make_float2(kk[2 * j], kk[2 * j + 1]);
-				S2[j] = __ffma2_rn(two2, K, S2[j]);
-				const float2 s = __ffma2_rn(hs2, K, H[j]);
-				t[2 * j] = s.x;
-				t[2 * j + 1] = s.y;
-			}
-			rhs<V, NF>(rc, t, kk);
-			const float2 h62 = make_float2(hs * (1.0f / 6.0f), hs * (1.0f / 6.0f));
-#pragma unroll
-			for(int j = 0; j < NP; ++j) {
-				const float2 K   = make_float2(kk[2 * j], kk[2 * j + 1]);
-				const float2 inc = __fmul2_rn(h62, __fadd2_rn(S2[j], K));
-				const float2 yv  = sub2(inc, make_float2(lo[2 * j], lo[2 * j + 1]));
-				const float2 tv  = __fadd2_rn(H[j], yv);
-				const float2 c   = sub2(sub2(tv, H[j]), yv);
-				hi[2 * j] = tv.x;
-				hi[2 * j + 1] = tv.y;
-				lo[2 * j] = c.x;
-				lo[2 * j + 1] = c.y;
-			}
+			rk4_packed<V, NF>(rc, hi, lo, hs);
 		} else {
-			V kk[ND], t[ND], sum[ND];
+			const V hh = bc<V>(0.5f) * hs;
+			V kk[NI], t[NI], sum[NI];
 			rhs<V, NF>(rc, hi, kk);
 #pragma unroll
-			for(int i = 0; i < ND; ++i) {
+			for(int i = 0; i < NI; ++i) {
 				sum[i] = kk[i];
 				t[i] = fmav(hh, kk[i], hi[i]);
 			}
 			rhs<V, NF>(rc, t, kk);
 #pragma unroll
-			for(int i = 0; i < ND; ++i) {
+			for(int i = 0; i < NI; ++i) {
 				sum[i] = fmav(bc<V>(2.0f), kk[i], sum[i]);
 				t[i] = fmav(hh, kk[i], hi[i]);
 			}
 			rhs<V, NF>(rc, t, kk);
 #pragma unroll
-			for(int i = 0; i < ND; ++i) {
+			for(int i = 0; i < NI; ++i) {
 				sum[i] = fmav(bc<V>(2.0f), kk[i], sum[i]);
 				t[i] = fmav(hs, kk[i], hi[i]);
 			}
 			rhs<V, NF>(rc, t, kk);
 			const V h6 = hs * bc<V>(1.0f / 6.0f);
 #pragma unroll
-			for(int i = 0; i < ND; ++i) {
+			for(int i = 0; i < NI; ++i) {
 				V inc = h6 * (sum[i] + kk[i]);
 				/* Kahan: value = hi - lo */
 				V yv = inc - lo[i];
@@ -694,7 +791,7 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 			s.h += dh[k];
 			if(s.h >= s.n) {
 				if(++s.dump >= s.dump_end) {
-					store_slot<V, ND>(s, k, hi, lo);
+					store_slot<V, NF>(s, k, hi, lo);
 					s.active = false;
 				} else {
 					start_dump(s);

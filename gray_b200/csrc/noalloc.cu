@@ -81,7 +81,7 @@ gray_run_mixed_noalloc(int device, const gray_render_desc *descs, int n_renders,
 		if(d.spacetime != GRAY_ST_KERR || d.n_freq != descs[0].n_freq ||
 		   d.flow != descs[0].flow || !state_dev[i] || !info_dev[i])
 			return GRAY_EINVAL;
-		total += (unsigned long long)d.n_width * d.n_height;
+		total += (unsigned long long)d.n_width * (d.n_rows ? d.n_rows : d.n_height);
 	}
 	if(total > (1ull << 31))
 		return GRAY_EINVAL; /* the ray queue is a 32-bit counter */

@@ -6,16 +6,19 @@ and copies are free.  Counts assume the ray is inside the emission region
 (r > r_isco, timelike Keplerian flow, shift > 0), which holds for nearly
 every step of the torus workloads; outside it the transfer part is skipped.
 
-Mixed kernel (gray_b200/csrc/kernels_mixed.cu), per call:
-  ks_rhs          166  (head 42: radius root, f and its gradient with
-                        2 rsqrt + 2 rcp; l and its gradient 33; the two
-                        contractions of d(f l.u l) taken directly, without
-                        the nine D_a^i, and the acceleration 91)
-  torus_rt        47 + 5 per frequency  (Keplerian flow 34, density 8 with
-                        1 ex2, j/shift^2 with lg2 + ex2 factored once, 1 ex2
-                        per frequency)
-  RK4 + Kahan     per component: stages 2 + 4 + 4, final 2 + 4 (Kahan)
-                  = 16, plus 3 scalars
+Mixed kernel (gray_b200/csrc/kernels_mixed.cu), per call; the geodesic is
+integrated in Hamiltonian form on (x^mu, k_i) with k_t conserved:
+  ks_ham          93   (head 32: radius root, f, df/dr and the explicit
+                        df/dz with 2 rsqrt + 2 rcp; l, L = l^mu k_mu,
+                        dL/dr and the force G d_i r + f L (explicit d_i L),
+                        and dx^mu/dl 61)
+  torus_rt        35 + 5 per frequency  (Keplerian flow and shift from
+                        k_mu 24, the density and dtau_0 folded into one
+                        ex2 11; per frequency one ex2 of the summed log2
+                        factors); only tau_0 is integrated, the other
+                        optical depths are (nu_0/nu_i)^2 times it
+  RK4 + Kahan     per integrated real: stages 2 + 4 + 4, final 2 + 4
+                  (Kahan) = 16, plus 3 scalars; 7 + (n_freq + 1) reals
   step control    17  (FP32 radius root and the n/|dt| tick rule)
 
 FP64 kernel (gray_b200/csrc/kernels_fp64.cu), per call:
@@ -30,9 +33,9 @@ The reference's own comments count the same KS RHS as about 205 FLOP
 
 
 def mixed_per_step(n_freq, transfer=True):
-    nd = 8 + 2 * n_freq
-    rhs = 166 + ((47 + 5 * n_freq) if (transfer and n_freq) else 0)
-    return 4 * rhs + 16 * nd + 3 + 17
+    ni = 7 + (n_freq + 1 if n_freq else 0)
+    rhs = 93 + ((35 + 5 * n_freq) if (transfer and n_freq) else 0)
+    return 4 * rhs + 16 * ni + 3 + 17
 
 
 def fp64_per_step(n_freq, transfer=True):

@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define GRAY_ABI_VERSION 2
+#define GRAY_ABI_VERSION 3
 #define GRAY_MAX_FREQ    8
 
 enum gray_status {
@@ -107,6 +107,14 @@ typedef struct gray_render_desc {
 	double   m_adm;           /* param.opts M_ADM:m, solar masses            */
 	double   flow_te;         /* electron temperature kT/(m_e c^2) (1e12)     */
 	double   flow_b;          /* magnetic field magnitude, along z (0)        */
+	/* camera row window (no reference counterpart): the render integrates
+	 * rows [row_begin, row_begin + n_rows) of the n_height-row image, with
+	 * the pixel map of the whole image (driver.cl:47-51), so that row
+	 * blocks of one render can run on different GPUs.  n_rows = 0 means
+	 * every row (row_begin must then be 0).  Ray r of the render is pixel
+	 * (r % n_width, row_begin + r / n_width). */
+	uint64_t row_begin;
+	uint64_t n_rows;
 } gray_render_desc;
 
 typedef struct gray_ctx gray_ctx;

@@ -109,6 +109,12 @@ int64_t orc_evolve_ray(const orc_desc *d, double *s, double dt, int64_t n_sub);
 int    orc_trace(const orc_desc *d, const int64_t *rays, int64_t n,
                  double *out, double *info, int64_t *steps, int nthreads);
 
+/* the same trace with every real in float (the reference's default
+ * precision, sim-org/setup.opts:6), gray_oracle32.c: the single-precision
+ * CPU baseline; out is [k][n_data] doubles, steps is [k] */
+int    orc32_trace(const orc_desc *d, const int64_t *rays, int64_t n,
+                   double *out, int64_t *steps, int nthreads);
+
 /* same, but only n_dump intervals starting from given states (in/out). */
 int    orc_evolve_states(const orc_desc *d, double *states, int64_t n,
                          double *info, int64_t *steps, int nthreads);

@@ -88,6 +88,8 @@ def lib():
         L.orc_evolve_ray.argtypes = [P(OrcDesc), pd, d, i64]
         L.orc_trace.restype = ctypes.c_int
         L.orc_trace.argtypes = [P(OrcDesc), pi64, i64, pd, pd, pi64, ctypes.c_int]
+        L.orc32_trace.restype = ctypes.c_int
+        L.orc32_trace.argtypes = [P(OrcDesc), pi64, i64, pd, pi64, ctypes.c_int]
         L.orc_evolve_states.restype = ctypes.c_int
         L.orc_evolve_states.argtypes = [P(OrcDesc), pd, i64, pd, pi64, ctypes.c_int]
         L.orc_rplus.restype = d
@@ -184,6 +186,20 @@ def trace(cfg, rays, nthreads=0):
     if rc != 0:
         raise ValueError("oracle rejected the configuration")
     return out, info, steps
+
+
+def trace32(cfg, rays, nthreads=0):
+    """The analytic trace with every real in float (gray_oracle32.c, the
+    single-precision CPU baseline).  Returns (states [n, n_data], steps [n])."""
+    L = lib()
+    d = make_desc(cfg)
+    rays = np.ascontiguousarray(rays, dtype=np.int64)
+    n = rays.size
+    out = np.zeros((n, n_data(cfg)))
+    steps = np.zeros(n, dtype=np.int64)
+    if L.orc32_trace(ctypes.byref(d), _pi(rays), n, _p(out), _pi(steps), nthreads) != 0:
+        raise ValueError("oracle rejected the configuration")
+    return out, steps
 
 
 def icond(cfg, rays):

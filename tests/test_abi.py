@@ -27,7 +27,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_strerror_and_version():
-    assert api.lib().gray_abi_version() == api.ABI_VERSION == 2
+    assert api.lib().gray_abi_version() == api.ABI_VERSION == 3
     assert api.strerror(api.EINVAL).startswith("invalid")
     assert api.strerror(api.EBUDGET).startswith("request exceeds")
     assert api.strerror(12345) == "unknown status"

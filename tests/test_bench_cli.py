@@ -17,7 +17,7 @@ def run(args, env=None):
 
 
 def test_reference_arm_line():
-    p = run(["--impl", "reference", "--steps", "1", "--warmup", "3", "--cpu-seconds", "0.2"])
+    p = run(["--impl", "reference", "--steps", "2", "--warmup", "3", "--cpu-rays", "64"])
     assert p.returncode == 0, p.stderr[-2000:]
     line = json.loads(p.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["metric"] == "ray-steps/s"

@@ -136,3 +136,34 @@ def test_mixed_matches_oracle_geodesics(ctx):
     print("mixed vs oracle: pos %.3e mom %.3e" % (pos, mom))
     assert pos <= 1e-4 and mom <= 1e-4
     assert abs(smx - osteps.sum()) <= 1e-3 * osteps.sum()
+
+
+@pytest.mark.parametrize("precision", [api.PREC_FP64, api.PREC_MIXED])
+def test_row_blocks_concatenate_to_the_render(ctx, precision):
+    """A render split into camera row windows (the multi-GPU row partition
+    of one render) gives, block after block, exactly the whole render: rays
+    are independent and the window keeps the whole image's pixel map."""
+    from gray_b200 import shard
+    cfg = dict(configs.scaled(configs.TORUS_RT_1024, 24), n_height=19, n_dump=8,
+               precision=precision)
+    full, finfo, fsteps = run_gpu(ctx, cfg)
+    parts, infos, steps = [], [], 0
+    for rank in range(3):
+        begin, rows = shard.row_block(cfg["n_height"], rank, 3)
+        g, gi, s = run_gpu(ctx, dict(cfg, row_begin=begin, n_rows=rows))
+        assert g.shape[0] == rows * cfg["n_width"]
+        parts.append(g)
+        infos.append(gi)
+        steps += s
+    assert np.array_equal(np.concatenate(parts), full)
+    assert np.array_equal(np.concatenate(infos), finfo)
+    assert steps == fsteps
+
+
+def test_row_window_is_validated(ctx):
+    base = dict(configs.scaled(configs.KERR_SMALL_64, 8), precision=api.PREC_FP64)
+    for bad in (dict(row_begin=1, n_rows=0), dict(row_begin=8, n_rows=1),
+                dict(row_begin=6, n_rows=3)):
+        with pytest.raises(api.GrayError) as e:
+            ctx.render(dict(base, **bad))
+        assert e.value.status == api.EINVAL

@@ -100,3 +100,49 @@ def test_partition_is_deterministic_and_handles_edges():
     assert a == shard.partition([3, 3, 2, 2, 2], 2)
     with pytest.raises(ValueError):
         shard.partition([1], 0)
+
+
+def _rows_worker(rank, world, port, q):
+    """Each rank traces its row block of a small torus render with the CPU
+    oracle (standing in for its GPU), rank 0 gathers; the GPU side of the
+    row window is checked by test_row_blocks_concatenate_to_the_render."""
+    _init(rank, world, port)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as O
+    from gray_b200 import configs, shard
+    cfg = dict(configs.scaled(configs.TORUS_RT_1024, 6), n_width=7, n_height=5, n_dump=3)
+    begin, rows = shard.row_block(cfg["n_height"], rank, world)
+    rays = begin * cfg["n_width"] + np.arange(rows * cfg["n_width"], dtype=np.int64)
+    st, _, _ = O.trace(cfg, rays)
+    full = shard.gather_rows(dist, st.T, cfg["n_width"], cfg["n_height"])
+    blocks = [None] * world
+    dist.all_gather_object(blocks, (begin, rows))
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank == 0:
+        ref, _, _ = O.trace(cfg, np.arange(cfg["n_width"] * cfg["n_height"], dtype=np.int64))
+        q.put((blocks, bool(np.array_equal(full, ref.T)), full.shape))
+
+
+def test_row_partition_gathers_to_the_one_rank_layout():
+    world, port = 2, free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.SimpleQueue()
+    ps = [ctx.Process(target=_rows_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(120)
+        assert p.exitcode == 0
+    blocks, same, shape = q.get()
+    assert blocks == [(0, 3), (3, 2)]  # every row once, in rank order
+    assert same and shape == (16, 35)
+
+
+def test_row_block_edges():
+    from gray_b200 import shard
+    assert [shard.row_block(10, r, 3) for r in range(3)] == [(0, 4), (4, 3), (7, 3)]
+    assert [shard.row_block(2, r, 4) for r in range(4)] == [(0, 1), (1, 1), (2, 0), (2, 0)]
+    with pytest.raises(ValueError):
+        shard.row_block(4, 2, 2)

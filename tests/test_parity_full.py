@@ -1,0 +1,212 @@
+"""Parity at the workloads' real sizes, on samples of the real ray sets.
+
+The other parity tests run scaled-down cameras, whose pixels sit in other
+places.  Here every GPU render is the full-size workload -- torus_rt_1024
+(1024^2 rays, 4 frequencies), numerical_128 (the 128^3 two-level grid and
+the 512^2 camera) and full-size renders of the survey_256 batch -- and the
+CPU oracle traces a strided sample of the same ray indices (stride 7919, a
+prime, so the sample covers every part of the image), as driver.cl:36-108
+would over the whole NDRange.
+
+Tolerances: FP64 kernel vs oracle <= 1e-10 relative per ray and component
+(the geodesic columns are bit-identical; exp/pow in the transfer may differ
+in the last bit between CUDA and glibc).  Mixed precision vs FP64: image
+(I_nu) relative L2 error <= 1e-4 per frequency, on the full image and on the
+oracle's sample, and end positions <= 1e-4.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from gray_b200 import api, configs
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-10
+TOL_MIXED = 1e-4
+STRIDE = 7919
+
+
+def sample(n_rays, k):
+    """k distinct ray indices spread over the image (STRIDE is coprime to
+    every power-of-two ray count used here)."""
+    return (np.arange(k, dtype=np.int64) * STRIDE) % n_rays
+
+
+def render_full(ctx, cfg):
+    r = ctx.render(cfg)
+    try:
+        r.run()
+        data, info = r.state(api.LAYOUT_SOA)
+        return data, info, r.steps()
+    finally:
+        r.close()
+
+
+def image_err(got, ref):
+    return np.linalg.norm(got - ref) / np.linalg.norm(ref)
+
+
+# ------------------------------------------------------------ torus_rt_1024
+
+@pytest.fixture(scope="module")
+def torus(ctx):
+    cfg = configs.TORUS_RT_1024
+    s64, i64, n64 = render_full(ctx, dict(cfg, precision=api.PREC_FP64))
+    smx, imx, nmx = render_full(ctx, dict(cfg, precision=api.PREC_MIXED))
+    return cfg, (s64, i64, n64), (smx, imx, nmx)
+
+
+def test_torus_1024_fp64_matches_oracle_on_sample(torus):
+    cfg, (s64, i64, _), _ = torus
+    rays = sample(cfg["n_width"] * cfg["n_height"], 2048)
+    o, oinfo, _ = O.trace(cfg, rays)
+    g = s64[:, rays].T
+    geo = np.abs(g[:, :8] - o[:, :8]) / np.abs(o[:, :8]).max(axis=1, keepdims=True)
+    rt = np.abs(g[:, 8:] - o[:, 8:]) / np.maximum(np.abs(o[:, 8:]), 1e-30)
+    exact = np.mean(np.all(g[:, :8] == o[:, :8], axis=1))
+    print("torus_rt_1024 fp64 vs oracle, %d rays: geodesic bit-identical %.4f, max rel %.3e; "
+          "transfer max rel %.3e" % (rays.size, exact, geo.max(), rt.max()))
+    assert geo.max() <= TOL64
+    assert rt.max() <= TOL64
+    assert np.max(np.abs(i64[rays] - oinfo)) <= 1e-12 * max(1.0, np.max(np.abs(oinfo)))
+
+
+def test_torus_1024_mixed_image_error(torus):
+    cfg, (s64, _, n64), (smx, imx, nmx) = torus
+    nf = len(cfg["nu"])
+    errs = [image_err(smx[8 + i], s64[8 + i]) for i in range(nf)]
+    pos = image_err(smx[1:4], s64[1:4])
+    print("torus_rt_1024 mixed vs fp64, every ray: image rel L2 %s, end position %.3e, "
+          "ray-steps %d vs %d" % (["%.2e" % e for e in errs], pos, nmx, n64))
+    assert max(errs) <= TOL_MIXED
+    assert pos <= TOL_MIXED
+    assert abs(nmx - n64) <= 1e-3 * n64
+    # null constraint relative to |u|^2 (captured rays end with large u)
+    norm = np.sum(smx[4:8] ** 2, axis=0)
+    assert np.max(np.abs(imx) / norm) < 1e-5
+
+
+def test_torus_1024_mixed_matches_oracle_on_sample(torus):
+    cfg, _, (smx, _, _) = torus
+    rays = sample(cfg["n_width"] * cfg["n_height"], 1024)
+    o, _, _ = O.trace(cfg, rays)
+    g = smx[:, rays].T
+    nf = len(cfg["nu"])
+    errs = [image_err(g[:, 8 + i], o[:, 8 + i]) for i in range(nf)]
+    pos = image_err(g[:, 1:4], o[:, 1:4])
+    print("torus_rt_1024 mixed vs oracle, %d rays: image %s, end position %.3e"
+          % (rays.size, ["%.2e" % e for e in errs], pos))
+    assert max(errs) <= TOL_MIXED and pos <= TOL_MIXED
+
+
+# ------------------------------------------------------------ numerical_128
+
+def close_with_nans(g, o, tol):
+    """Same NaN/Inf pattern (rays that ran into the singular region compute
+    the same non-finite values on both sides); relative agreement on the
+    finite rays.  Returns (bit-identical fraction, max rel err)."""
+    fin = np.all(np.isfinite(o), axis=1)
+    assert np.array_equal(fin, np.all(np.isfinite(g), axis=1))
+    gg, oo = g[fin], o[fin]
+    err = np.max(np.abs(gg - oo) / np.abs(oo).max(axis=1, keepdims=True))
+    assert err <= tol, err
+    return np.mean(np.all(gg == oo, axis=1)), err
+
+
+@pytest.fixture(scope="module")
+def numerical(ctx):
+    G = configs.NUMERICAL_GRID
+    grid = api.make_grid(G["n"], -G["box"], G["box"], G["t1"], G["t2"], physics=True)
+    ctx.make_boosted_ks(grid, G["a"], G["v"], G["axis"], G["t1"], 0)
+    ctx.make_boosted_ks(grid, G["a"], G["v"], G["axis"], G["t2"], 1)
+    lv = [ctx.read_spacetime(grid, 0), ctx.read_spacetime(grid, 1)]
+    box = [G["t1"], -G["box"], -G["box"], -G["box"], G["t2"], G["box"], G["box"], G["box"]]
+    return G, grid, lv, box
+
+
+def test_numerical_128_fp64_matches_oracle_on_sample(ctx, numerical):
+    """Physics mode on the real grid and camera, as the throughput run."""
+    G, grid, lv, box = numerical
+    ctx.make_boosted_ks(grid, G["a"], G["v"], G["axis"], G["t1"], 0)  # physics-mode desc
+    ctx.make_boosted_ks(grid, G["a"], G["v"], G["axis"], G["t2"], 1)
+    cfg = configs.NUMERICAL_128
+    s64, _, _ = render_full(ctx, dict(cfg, precision=api.PREC_FP64))
+    rays = sample(cfg["n_width"] * cfg["n_height"], 384)
+    og = O.Grid(lv, box, physics=True)
+    o, _, _ = O.dyst_trace(cfg, og, rays)
+    exact, err = close_with_nans(s64[:, rays].T, o, TOL64)
+    print("numerical_128 fp64 vs oracle, %d rays: bit-identical %.4f, max rel %.3e"
+          % (rays.size, exact, err))
+
+
+def test_numerical_128_mixed_vs_fp64(ctx, numerical):
+    G, grid, _, _ = numerical
+    ctx.make_boosted_ks(grid, G["a"], G["v"], G["axis"], G["t1"], 0)
+    ctx.make_boosted_ks(grid, G["a"], G["v"], G["axis"], G["t2"], 1)
+    cfg = configs.NUMERICAL_128
+    s64, _, _ = render_full(ctx, dict(cfg, precision=api.PREC_FP64))
+    smx, _, _ = render_full(ctx, dict(cfg, precision=api.PREC_MIXED))
+    # the image is the rays that escape to 100..1000 M: the numerical
+    # spacetime has no horizon stop (dyst.cl:43-53), so captured rays run on
+    # inside the singular region where the precisions part ways
+    fin = np.all(np.isfinite(s64), axis=0) & np.all(np.isfinite(smx), axis=0)
+    rend = np.sqrt(np.sum(s64[1:4] ** 2, axis=0))
+    esc = fin & (rend > 100.0) & (rend < 1000.0)
+    err = image_err(smx[1:4, esc], s64[1:4, esc])
+    print("numerical_128 mixed vs fp64: escaping %.3f of %d rays, end position rel L2 %.3e"
+          % (esc.mean(), esc.size, err))
+    assert esc.mean() > 0.5
+    assert err <= TOL_MIXED
+
+
+def test_numerical_128_reference_semantics_in_box_camera(ctx, numerical):
+    """Reference semantics (clamp-to-edge outside the box, unclamped linear
+    time extrapolation) on the real 128^3 grid, with a camera inside the box
+    and |dt| within the levels, the regime where those semantics are
+    meaningful."""
+    G, _, lv, box = numerical
+    grid = api.make_grid(G["n"], -G["box"], G["box"], G["t1"], G["t2"], physics=False)
+    ctx.make_boosted_ks(grid, G["a"], G["v"], G["axis"], G["t1"], 0)
+    ctx.make_boosted_ks(grid, G["a"], G["v"], G["axis"], G["t2"], 1)
+    cfg = dict(configs.NUMERICAL_128, r_obs=30.0, w_img=30.0, h_img=30.0, n_width=128,
+               n_height=128, dt_dump=-2.0, n_dump=5, t_init=0.0)
+    s64, _, _ = render_full(ctx, dict(cfg, precision=api.PREC_FP64))
+    rays = sample(128 * 128, 512)
+    og = O.Grid(lv, box, physics=False)
+    o, _, _ = O.dyst_trace(cfg, og, rays)
+    exact, err = close_with_nans(s64[:, rays].T, o, TOL64)
+    print("numerical_128 reference semantics, in-box camera, %d rays: bit-identical %.4f, "
+          "max rel %.3e" % (rays.size, exact, err))
+
+
+# --------------------------------------------------------------- survey_256
+
+def test_survey_full_size_renders_batched_vs_fp64_alone(ctx):
+    """Eight full-size renders of the survey (its first eight, as seeded),
+    batched in one persistent launch in mixed precision, against each render
+    run alone in FP64; the FP64 renders against the oracle on a sample."""
+    cfgs = configs.survey()[:8]
+    rs = [ctx.render(dict(c, precision=api.PREC_MIXED)) for c in cfgs]
+    b = ctx.batch(rs)
+    try:
+        b.run()
+        for k, (r, c) in enumerate(zip(rs, cfgs)):
+            s64, _, _ = render_full(ctx, dict(c, precision=api.PREC_FP64))
+            got = r.state(api.LAYOUT_SOA)[0]
+            errs = [image_err(got[8 + i], s64[8 + i]) for i in range(len(c["nu"]))]
+            n_rays = c["n_width"] * c["n_height"]
+            rays = sample(n_rays, min(64, n_rays))
+            o, _, _ = O.trace(c, rays)
+            g = s64[:, rays].T
+            geo = np.max(np.abs(g[:, :8] - o[:, :8]) / np.abs(o[:, :8]).max(axis=1, keepdims=True))
+            rt = np.max(np.abs(g[:, 8:] - o[:, 8:]) / np.maximum(np.abs(o[:, 8:]), 1e-30))
+            print("survey render %d (%d^2, a=%.3f, i=%.1f, r=%.0f): batched mixed image %.2e; "
+                  "fp64 vs oracle geo %.1e rt %.1e" % (k, c["n_width"], c["a_spin"], c["i_obs"],
+                                                     c["r_obs"], max(errs), geo, rt))
+            assert max(errs) <= TOL_MIXED
+            assert geo <= TOL64 and rt <= TOL64
+    finally:
+        b.close()
+        for r in rs:
+            r.close()
