@@ -346,17 +346,147 @@ dyst_rhs32(const GridParams &g, const DystConst &dc, float4 *cells, const float 
 	}
 }
 
+/* ------------------------------------------ gathers staged in shared memory */
+
+/* The same geodesic RHS with the corner rows staged through shared memory:
+ * each (corner, level) row of 40 Gamma is copied global -> shared with ten
+ * 16-byte cp.async (through L1, .ca) into a per-thread double buffer, and
+ * the copy of the next row is in flight while the current one is
+ * contracted.  The loads then hold no registers while they wait, so more of
+ * them overlap than the register-resident form allows at 16 warps per SM.
+ * Buffer layout [stage][chunk][thread] of float4: a warp's LDS.128 of one
+ * chunk touches 32 consecutive float4, without bank conflicts. */
+constexpr int STAGE_CHUNKS = 10; /* 40 floats = 10 x 16 bytes */
+
+__device__ __forceinline__ void
+cp_async16(float4 *dst, const float *src)
+{
+	const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void
+cp_async_commit()
+{
+	asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void
+cp_async_wait()
+{
+	asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void
+dyst_rhs32_staged(const GridParams &g, const DystConst &dc, float4 *cells, float4 *stage,
+                  const float *s, float *ds)
+{
+	const float *u = s + 4;
+	ds[0] = u[0]; ds[1] = u[1]; ds[2] = u[2]; ds[3] = u[3];
+	if(g.physics && !inside32(g, s)) {
+		ds[4] = ds[5] = ds[6] = ds[7] = 0.0f;
+		return;
+	}
+	int i0[3], i1[3];
+	float w[3];
+	const int n[3] = {g.nx, g.ny, g.nz};
+#pragma unroll
+	for(int a = 0; a < 3; ++a) {
+		float uu = axis_uvw32c(g, a, s[a + 1], dc.B[a], dc.iA[a], cells[a * CELL_STRIDE]);
+		float fl = floorf(uu);
+		i0[a] = (int)fl;
+		w[a] = uu - fl;
+		i1[a] = min(i0[a] + 1, n[a] - 1);
+	}
+	float ft = 0.0f;
+	if(!g.single) {
+		ft = (s[0] - g.box[0]) * rcp_a(g.box[4] - g.box[0]);
+		if(g.physics)
+			ft = fminf(fmaxf(ft, 0.0f), 1.0f);
+	}
+	float p[10];
+	{
+		int k = 0;
+#pragma unroll
+		for(int i = 0; i < 4; ++i)
+#pragma unroll
+			for(int j = i; j < 4; ++j) {
+				float uu = u[i] * u[j];
+				p[k++] = i == j ? uu : 2.0f * uu;
+			}
+	}
+	float Gm[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+	const float ax = 1.0f - w[0], ay = 1.0f - w[1], az = 1.0f - w[2];
+	const bool use0 = g.single || ft < 1.0f;
+	const bool use1 = !g.single && ft > 0.0f;
+	/* the (corner, level) rows to gather: corner-major, levels in order */
+	const int nl = (use0 ? 1 : 0) + (use1 ? 1 : 0);
+	const int l0 = use0 ? 0 : 1;
+	const int items = 8 * nl;
+	auto row_of = [&](int it) {
+		const int c = it / nl, l = l0 + it % nl;
+		const int ix = (c & 1) ? i1[0] : i0[0];
+		const int iy = (c & 2) ? i1[1] : i0[1];
+		const int iz = (c & 4) ? i1[2] : i0[2];
+		return g.lvl[l] + (((long long)iz * g.ny + iy) * g.nx + ix) * GRAY_NSTRIDE;
+	};
+	auto issue = [&](int it) {
+		const float *src = row_of(it);
+		float4 *dst = stage + (it & 1) * STAGE_CHUNKS * CELL_STRIDE;
+#pragma unroll
+		for(int k = 0; k < STAGE_CHUNKS; ++k)
+			cp_async16(dst + k * CELL_STRIDE, src + 4 * k);
+		cp_async_commit();
+	};
+	issue(0);
+#pragma unroll 1
+	for(int it = 0; it < items; ++it) {
+		if(it + 1 < items) {
+			issue(it + 1);
+			cp_async_wait<1>(); /* row it has landed, row it + 1 in flight */
+		} else {
+			cp_async_wait<0>();
+		}
+		const int c = it / nl, l = l0 + it % nl;
+		float wl = ((c & 1) ? w[0] : ax) * ((c & 2) ? w[1] : ay) * ((c & 4) ? w[2] : az);
+		if(!g.single)
+			wl *= l ? ft : 1.0f - ft;
+		const float4 *src = stage + (it & 1) * STAGE_CHUNKS * CELL_STRIDE;
+		float sm[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+		for(int k = 0; k < STAGE_CHUNKS; ++k) {
+			const float4 v = src[k * CELL_STRIDE];
+			const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+			for(int q = 0; q < 4; ++q) {
+				const int idx = 4 * k + q; /* Gamma^(idx/10)_(idx%10) */
+				sm[idx / 10] = fmaf(vv[q], p[idx % 10], sm[idx / 10]);
+			}
+		}
+#pragma unroll
+		for(int m = 0; m < 4; ++m)
+			Gm[m] = fmaf(wl, sm[m], Gm[m]);
+	}
+#pragma unroll
+	for(int m = 0; m < 4; ++m)
+		ds[4 + m] = fmaf(Gm[0], u[m], -Gm[m]);
+}
+
 /* NF > 0: the thermal transfer pairs (I, tau) ride along in FP64 (rt[],
  * first the NF intensities, then the NF optical depths), integrated by the
  * same RK4 stages with the FP64 emissivities of thermal.cuh on the FP32
  * momentum and density; the stages run as a rolled loop so that the FP64
  * transfer is instantiated once. */
-template <int NF>
+template <int NF, bool STAGED>
 __global__ void __launch_bounds__(256, NF == 0 ? 2 : 1)
 dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
                   unsigned int *__restrict__ queue, unsigned long long *__restrict__ steps,
                   unsigned long long *__restrict__ inbox)
 {
+	static_assert(!STAGED || NF == 0, "staged gathers: geodesic-only renders");
+	extern __shared__ float4 s_stage[]; /* STAGED: 2 x STAGE_CHUNKS x CELL_STRIDE */
+	float4 *stage = s_stage + threadIdx.x;
 	constexpr int ND = 8;            /* FP32 geodesic state           */
 	constexpr int NR = 2 * NF;       /* FP64 transfer state           */
 	const unsigned FULL = 0xffffffffu;
@@ -482,25 +612,31 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 			for(int i = 0; i < NR; ++i)
 				rt[i] = fma(hsd / 6.0, srt[i], rt[i]);
 		} else {
-		dyst_rhs32(g, dc, cells, hi, k);
+		auto geo = [&](const float *sv, float *kv) {
+			if constexpr(STAGED)
+				dyst_rhs32_staged(g, dc, cells, stage, sv, kv);
+			else
+				dyst_rhs32(g, dc, cells, sv, kv);
+		};
+		geo(hi, k);
 #pragma unroll
 		for(int i = 0; i < ND; ++i) {
 			sum[i] = k[i];
 			t[i] = fmaf(hh, k[i], hi[i]);
 		}
-		dyst_rhs32(g, dc, cells, t, k);
+		geo(t, k);
 #pragma unroll
 		for(int i = 0; i < ND; ++i) {
 			sum[i] = fmaf(2.0f, k[i], sum[i]);
 			t[i] = fmaf(hh, k[i], hi[i]);
 		}
-		dyst_rhs32(g, dc, cells, t, k);
+		geo(t, k);
 #pragma unroll
 		for(int i = 0; i < ND; ++i) {
 			sum[i] = fmaf(2.0f, k[i], sum[i]);
 			t[i] = fmaf(hs, k[i], hi[i]);
 		}
-		dyst_rhs32(g, dc, cells, t, k);
+		geo(t, k);
 		}
 		const float h6 = hs * (1.0f / 6.0f);
 		bool bad = false;
@@ -540,19 +676,27 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 		atomicAdd(inbox, cnt_in);
 }
 
-template <int NF>
+template <int NF, bool STAGED>
 cudaError_t
-launch_dyst_nf(const MixedTable &T, const GridParams &g, const DystConst &dc,
-               unsigned int *queue, unsigned long long *steps, cudaStream_t st,
-               const MixedLaunch &cfg, unsigned long long *inbox)
+launch_dyst_nfs(const MixedTable &T, const GridParams &g, const DystConst &dc,
+                unsigned int *queue, unsigned long long *steps, cudaStream_t st,
+                const MixedLaunch &cfg, unsigned long long *inbox)
 {
 	int block = cfg.block > 0 ? cfg.block : 256;
 	if(block > 256)
 		return cudaErrorInvalidValue; /* __launch_bounds__(256) */
+	/* the stage is indexed with the CELL_STRIDE of the launch bound */
+	const size_t smem = STAGED ? 2 * STAGE_CHUNKS * CELL_STRIDE * sizeof(float4) : 0;
+	cudaError_t e = cudaSuccess;
+	if(STAGED)
+		e = cudaFuncSetAttribute(dyst_mixed_kernel<NF, STAGED>,
+		                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	if(e != cudaSuccess)
+		return e;
 	int per_sm = cfg.blocks_per_sm;
 	if(per_sm <= 0) {
-		cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-			&per_sm, dyst_mixed_kernel<NF>, block, 0);
+		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dyst_mixed_kernel<NF, STAGED>,
+		                                                  block, smem);
 		if(e != cudaSuccess)
 			return e;
 		if(per_sm <= 0)
@@ -563,8 +707,24 @@ launch_dyst_nf(const MixedTable &T, const GridParams &g, const DystConst &dc,
 	unsigned grid = (unsigned)(want < need ? want : need);
 	if(grid == 0)
 		grid = 1;
-	dyst_mixed_kernel<NF><<<grid, block, 0, st>>>(T, g, dc, queue, steps, inbox);
+	dyst_mixed_kernel<NF, STAGED><<<grid, block, smem, st>>>(T, g, dc, queue, steps, inbox);
 	return cudaGetLastError();
+}
+
+#ifndef GRAY_DYST_STAGED
+#define GRAY_DYST_STAGED 0
+#endif
+
+template <int NF>
+cudaError_t
+launch_dyst_nf(const MixedTable &T, const GridParams &g, const DystConst &dc,
+               unsigned int *queue, unsigned long long *steps, cudaStream_t st,
+               const MixedLaunch &cfg, unsigned long long *inbox)
+{
+	if constexpr(NF == 0)
+		if(GRAY_DYST_STAGED)
+			return launch_dyst_nfs<0, true>(T, g, dc, queue, steps, st, cfg, inbox);
+	return launch_dyst_nfs<NF, false>(T, g, dc, queue, steps, st, cfg, inbox);
 }
 
 } /* namespace */

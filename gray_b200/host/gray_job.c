@@ -22,9 +22,17 @@
  * init() replaces sim/gray.c:75-151 (device, ray buffer, initcond, planner);
  * exec() replaces the dump loop of sim-org/gray.c:243-294 with the per-dump
  * evolve the new tree leaves as a TODO (sim/gray.c:168), and writes the raw
- * dumps of sim-org/io.c:39-72.
+ * dumps of sim-org/io.c:39-72 (outfile) and the HDF5 /rays files of
+ * sim/gray.c:170-176 (rayfile); either is switched off by an empty name.
+ *
+ * spacetime=dyst is the numerical spacetime of sim-org (dyst.cl, built in
+ * place of KS.cl there): the snapshots come from the HDF5 file dyst_file
+ * (sim-org/gray.c:164-230, io.c:149-533) and stream through
+ * gray_run_series, one snapshot pair per dump interval as
+ * sim-org/gray.c:243-294 switches them.
  */
 #include "gray_job.h"
+#include "gray_h5.h"
 
 #include <errno.h>
 #include <math.h>
@@ -76,6 +84,8 @@ struct gray_job {
 	/* run time */
 	gray_ctx *ctx;
 	int       render;
+	gray_h5_spacetime *sf;   /* spacetime=dyst: the open dyst_file */
+	gray_grid_desc     grid;
 	uint64_t  steps;
 	double    ns;
 };
@@ -285,7 +295,7 @@ valid_pattern(const char *s)
 static int
 valid_choices(const struct gray_job *j)
 {
-	if(strcmp(j->spacetime, "Kerr") && strcmp(j->spacetime, "KS"))
+	if(strcmp(j->spacetime, "Kerr") && strcmp(j->spacetime, "KS") && strcmp(j->spacetime, "dyst"))
 		return 0; /* sim/gray.c:55-57: unknown spacetime */
 	if(strcmp(j->initcond, "infcam"))
 		return 0; /* sim/gray.c:67-69: unknown initial conditions */
@@ -293,7 +303,7 @@ valid_choices(const struct gray_job *j)
 		return 0; /* sim-org/setup.opts:7: the only scheme shipped */
 	if(strcmp(j->morder, "AoS") && strcmp(j->morder, "SoA"))
 		return 0;
-	if(strcmp(j->flow, "torus") && strcmp(j->flow, "none"))
+	if(strcmp(j->flow, "torus") && strcmp(j->flow, "none") && strcmp(j->flow, "thermal"))
 		return 0;
 	if(strcmp(j->term, "eps") && strcmp(j->term, "rplus"))
 		return 0;
@@ -358,7 +368,7 @@ gray_job_desc(const gray_lux_job *ego, gray_render_desc *d)
 	d->torus_n0 = j->torus_n0;
 	d->torus_kappa = j->torus_kappa;
 	d->torus_hr = j->torus_hr;
-	d->spacetime = GRAY_ST_KERR;
+	d->spacetime = strcmp(j->spacetime, "dyst") ? GRAY_ST_KERR : GRAY_ST_NUMERICAL;
 	d->precision = j->precision == 8 ? GRAY_PREC_FP64 : GRAY_PREC_MIXED;
 	return GRAY_OK;
 }
@@ -497,6 +507,44 @@ resume(struct gray_job *j, size_t i)
 	return st;
 }
 
+/* sim/gray.c:170-176: after interval i (>= 1) the rays, copied to the host
+ * as an array {n_width, n_height, n_data} of the run's real type, go to a
+ * new HDF5 file rayfile % i as the dataset /rays (never overwritten: the
+ * reference opens it with H5F_ACC_EXCL) */
+static int
+dump_rays(struct gray_job *j, size_t i)
+{
+	if(!j->rayfile[0])
+		return GRAY_OK;
+	gray_render_desc d;
+	gray_job_desc(&j->super, &d);
+	const size_t n_rays = d.n_width * d.n_height;
+	const size_t n_data = 8 + 2 * (size_t)d.n_freq, n = n_rays * n_data;
+	double *data = malloc(sizeof(double) * n);
+	double *info = malloc(sizeof(double) * n_rays);
+	int st = (data && info) ? GRAY_OK : GRAY_ENOMEM;
+	if(!st)
+		st = gray_read_state(j->ctx, j->render, data, sizeof(double) * n, info,
+		                     sizeof(double) * n_rays, GRAY_LAYOUT_AOS);
+	if(!st) {
+		char name[512];
+		snprintf(name, sizeof(name), j->rayfile, (int)i);
+		const int sz = (int)dump_size(j);
+		if(sz == (int)sizeof(float)) {
+			float *f = (float *)data; /* narrowed in place, front to back */
+			for(size_t k = 0; k < n; ++k)
+				f[k] = (float)data[k];
+		}
+		int h = gray_h5_write_rays(name, data, sz, d.n_width, d.n_height, n_data);
+		st = h == GRAY_H5_OK ? GRAY_OK : h == GRAY_H5_EEXIST ? GRAY_ESTATE : GRAY_EINVAL;
+		if(h)
+			fprintf(stderr, "GRay2: %s: %s\n", name, gray_h5_strerror(h));
+	}
+	free(data);
+	free(info);
+	return st;
+}
+
 /* sim-org/io.c:39-72 dump(): header {sz, n_data, W, H}, the state, its
  * info diagnostic, in the run's element size and memory order */
 static int
@@ -540,7 +588,39 @@ dump(struct gray_job *j, size_t i)
 	}
 	free(data);
 	free(info);
+	if(!st && i > 0)
+		st = dump_rays(j, i);
 	return st;
+}
+
+/* sim-org/gray.c:164-205 + io.c:149-275: open dyst_file, list its
+ * snapshot times and read the grid; the grid keeps the reference's
+ * semantics (clamp-to-edge outside the box, unclamped time extrapolation) */
+static int
+open_dyst(struct gray_job *j)
+{
+	int h = gray_h5_spacetime_open(j->dyst_file, &j->sf);
+	if(h) {
+		fprintf(stderr, "GRay2: %s: %s\n", j->dyst_file, gray_h5_strerror(h));
+		return h == GRAY_H5_ENOTFOUND ? GRAY_ENOTFOUND : GRAY_EINVAL;
+	}
+	const double *times;
+	uint64_t nt = gray_h5_spacetime_times(j->sf, &times);
+	int n[3];
+	float lo[3], hi[3];
+	gray_h5_spacetime_grid(j->sf, n, lo, hi);
+	memset(&j->grid, 0, sizeof(j->grid));
+	j->grid.nx = n[0];
+	j->grid.ny = n[1];
+	j->grid.nz = n[2];
+	for(int a = 0; a < 3; ++a) {
+		j->grid.box[1 + a] = lo[a];
+		j->grid.box[5 + a] = hi[a];
+	}
+	printf("GRay2: Reading spacetime from file %s: %llu snapshot(s) in [%g, %g], "
+	       "grid %dx%dx%d\n", j->dyst_file, (unsigned long long)nt, times[0], times[nt - 1],
+	       n[0], n[1], n[2]);
+	return GRAY_OK;
 }
 
 static int
@@ -554,6 +634,11 @@ init(gray_lux_job *ego)
 		gray_destroy(EGO->ctx);
 		EGO->ctx = NULL;
 	}
+	gray_h5_spacetime_close(EGO->sf);
+	EGO->sf = NULL;
+	/* the spacetime file first: a bad file needs no device to be refused */
+	if(d.spacetime == GRAY_ST_NUMERICAL && (st = open_dyst(EGO)))
+		return st;
 	EGO->ctx = gray_create((int)EGO->i_device, 0, &st);
 	if(!EGO->ctx)
 		return st;
@@ -563,7 +648,8 @@ init(gray_lux_job *ego)
 	/* the lux planner of sim/gray/Kerr/ocl.c:41-75: time the launch shapes
 	 * on this render (a mixed one: the FP64 kernel has a single shape);
 	 * exec starts from icond, so the trial launches leave no trace */
-	if(d.precision == GRAY_PREC_MIXED && !strcmp(EGO->plan, "measure")) {
+	if(d.precision == GRAY_PREC_MIXED && d.spacetime == GRAY_ST_KERR &&
+	   !strcmp(EGO->plan, "measure")) {
 		int batch;
 		gray_launch_plan best;
 		if((st = gray_batch_create(EGO->ctx, &EGO->render, 1, &batch)))
@@ -580,6 +666,84 @@ init(gray_lux_job *ego)
 	return GRAY_OK;
 }
 
+typedef struct {
+	struct gray_job *j;
+	const double    *times;
+	size_t           i;
+} series_user;
+
+static int
+series_load(void *user, uint64_t k, float *fields)
+{
+	series_user *u = (series_user *)user;
+	return gray_h5_spacetime_load(u->j->sf, k, fields) != GRAY_H5_OK;
+}
+
+static int
+series_dump(void *user, uint64_t i)
+{
+	series_user *u = (series_user *)user;
+	struct gray_job *j = u->j;
+	printf("%llu: %4.1f -> %4.1f", (unsigned long long)i,
+	       j->t_init + (double)(i - 1) * j->dt_dump, j->t_init + (double)i * j->dt_dump);
+	int st = dump(j, i);
+	printf(st ? ": FAILED\n" : ": DONE\n");
+	return st != GRAY_OK;
+}
+
+/* sim-org/gray.c:164-294 with spacetime=dyst: icond on the snapshot pair
+ * bracketing t_init, dump 0, then the dump intervals with their snapshot
+ * pairs streamed by gray_run_series (which repeats the icond on the same
+ * pair: the state it integrates is the one dumped).  The reference has no
+ * restart from a dump on this path, and neither has the job: i_init must
+ * be 0. */
+static int
+exec_dyst(struct gray_job *j)
+{
+	const double *times;
+	const uint64_t nt = gray_h5_spacetime_times(j->sf, &times);
+	if(j->i_init)
+		return GRAY_EINVAL;
+	int64_t first;
+	int st = gray_series_schedule(times, nt, j->t_init, j->dt_dump, 1, (int)j->enable_fast_light,
+	                              &first);
+	if(st)
+		return st;
+	const int frozen = nt == 1 || j->enable_fast_light;
+	const size_t npts = (size_t)j->grid.nx * j->grid.ny * j->grid.nz;
+	float *lv = malloc(sizeof(float) * npts * 51);
+	if(!lv)
+		return GRAY_ENOMEM;
+	gray_grid_desc g = j->grid;
+	g.box[0] = (float)times[first];
+	g.box[4] = (float)times[frozen ? first : first + 1];
+	for(int l = 0; l < 2 && !st; ++l) {
+		int h = gray_h5_spacetime_load(j->sf, (uint64_t)(l && !frozen ? first + 1 : first), lv);
+		st = h ? GRAY_ESOURCE : gray_load_spacetime_interleaved(j->ctx, &g, lv, l);
+	}
+	free(lv);
+	if(!st)
+		st = gray_icond(j->ctx, j->render);
+	if(st)
+		return st;
+	printf("0:  initialize at %4.1f", j->t_init);
+	if((st = dump(j, 0)))
+		return st;
+	printf(": DONE\n");
+	series_user u = {j, times, 0};
+	gray_snapshot_source src = {nt, times, &u, series_load};
+	uint64_t loads = 0;
+	double ns = 0.0;
+	st = gray_run_series(j->ctx, j->render, &j->grid, &src, (int)j->enable_fast_light,
+	                     series_dump, &ns, &loads);
+	if(st)
+		return st;
+	j->ns += ns;
+	printf("GRay2: %llu snapshot load(s)\n", (unsigned long long)loads);
+	fflush(stdout);
+	return gray_ray_steps(j->ctx, j->render, &j->steps);
+}
+
 /* sim-org/gray.c:243-294 */
 static int
 exec(gray_lux_job *ego)
@@ -588,6 +752,8 @@ exec(gray_lux_job *ego)
 	size_t i = j->i_init;
 	if(!j->ctx)
 		return GRAY_ESTATE;
+	if(j->sf)
+		return exec_dyst(j);
 	const double n_rays = (double)j->n_width * (double)j->n_height;
 	int st = resume(j, i);
 	if(st == GRAY_OK) {
@@ -643,5 +809,6 @@ gray_job_rmmod(gray_lux_job *ego)
 		return;
 	if(EGO->ctx)
 		gray_destroy(EGO->ctx); /* frees the render as well */
+	gray_h5_spacetime_close(EGO->sf);
 	free(ego);
 }

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from gray_b200 import api
+from gray_b200 import api, h5
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB = os.path.join(ROOT, "gray_b200", "lib", "libgray_job.so")
@@ -35,11 +35,17 @@ class Job:
         self.h = L.gray_job_mkmod(None)
         assert self.h
         CONF = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_char_p)
-        # struct gray_lux_job: the vtable is the first member
-        self.conf_fn = CONF(ctypes.cast(self.h, ctypes.POINTER(ctypes.c_void_p))[0])
+        RUN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)
+        # struct gray_lux_job: the vtable {conf, init, exec} is the first member
+        vt = ctypes.cast(self.h, ctypes.POINTER(ctypes.c_void_p))
+        self.conf_fn = CONF(vt[0])
+        self.init_fn = RUN(vt[1])
 
     def conf(self, arg):
         return self.conf_fn(self.h, arg.encode())
+
+    def init(self):
+        return self.init_fn(self.h)
 
     def get(self, name):
         buf = ctypes.create_string_buffer(512)
@@ -161,8 +167,10 @@ def read_raw(path):
 @pytest.mark.gpu
 def test_cli_dumps_match_oracle(tmp_path):
     args = ["a=0.9", "r=1000", "i=60", "w=40", "h=40", "W=12", "H=10", "dt=-31.25",
-            "n=1000", "N=3", "p=8", "out=" + str(tmp_path / "%04d.raw")]
-    res = subprocess.run([CLI] + args, capture_output=True, text=True, timeout=300)
+            "n=1000", "N=3", "p=8", "out=" + str(tmp_path / "%04d.raw"),
+            "ray=" + str(tmp_path / "ray%04d.h5")]
+    res = subprocess.run([CLI] + args, capture_output=True, text=True, timeout=300,
+                         cwd=tmp_path)
     assert res.returncode == 0, res.stderr
     assert "3: -62.5 -> -93.8: DONE" in res.stdout
     cfg = dict(a_spin=0.9, r_obs=1000.0, i_obs=60.0, w_img=40.0, h_img=40.0, n_width=12,
@@ -175,6 +183,13 @@ def test_cli_dumps_match_oracle(tmp_path):
             ref, _, _ = O.trace(dict(cfg, n_dump=i), np.arange(120))
         assert np.array_equal(data, ref), i
         assert np.max(np.abs(info)) < 1e-9
+        # sim/gray.c:170-176: the same rays in /rays of ray%04d.h5 after each interval
+        ray = tmp_path / ("ray%04d.h5" % i)
+        assert ray.exists() == (i > 0)
+        if i > 0:
+            with h5.File(str(ray)) as f:
+                assert f.info("rays") == ((12, 10, 8), 8)
+                assert np.array_equal(f.read("rays").reshape(120, 8), data)
 
 
 @pytest.mark.gpu
@@ -183,7 +198,7 @@ def test_cli_resumes_from_a_dump(tmp_path):
     the uninterrupted run's, bit for bit; without the file the run starts
     from the camera as the reference does."""
     common = ["a=0.9", "r=1000", "i=60", "w=40", "h=40", "W=8", "H=6", "dt=-31.25",
-              "n=1000", "N=4", "p=8"]
+              "n=1000", "N=4", "p=8", "ray="]
     full, part = tmp_path / "full", tmp_path / "part"
     full.mkdir()
     part.mkdir()
@@ -213,7 +228,8 @@ def test_cli_dump_follows_precision_and_memory_order(tmp_path):
     for mo in ("AoS", "SoA"):
         d = tmp_path / mo
         d.mkdir()
-        res = subprocess.run([CLI] + common + ["mo=" + mo, "out=" + str(d / "%04d.raw")],
+        res = subprocess.run([CLI] + common + ["mo=" + mo, "out=" + str(d / "%04d.raw"),
+                                               "ray=" + str(d / "ray%04d.h5")],
                              capture_output=True, text=True, timeout=300)
         assert res.returncode == 0, res.stderr
         raw = (d / "0002.raw").read_bytes()
@@ -222,6 +238,10 @@ def test_cli_dump_follows_precision_and_memory_order(tmp_path):
         body = np.frombuffer(raw[32:], dtype=np.float32)
         assert body.size == 48 * 8 + 48
         out[mo] = body[:48 * 8], body[48 * 8:]
+    with h5.File(str(tmp_path / "SoA" / "ray0002.h5")) as f:
+        assert f.info("rays") == ((8, 6, 8), 4)  # the run's real: float for p=4
+        assert np.array_equal(f.read("rays", np.float32).reshape(48, 8),
+                              out["AoS"][0].reshape(48, 8))
     aos, soa = out["AoS"][0].reshape(48, 8), out["SoA"][0].reshape(8, 48)
     assert np.array_equal(aos, soa.T) and np.array_equal(out["AoS"][1], out["SoA"][1])
     # and the numbers are the mixed render's, rounded to float
@@ -230,3 +250,49 @@ def test_cli_dump_follows_precision_and_memory_order(tmp_path):
     ref, _, _ = O.trace(cfg, np.arange(48))
     scale = np.abs(ref).max(axis=1, keepdims=True)
     assert np.max(np.abs(aos - ref) / scale) <= 1e-4
+
+
+def test_dyst_options_and_file_checks_need_no_gpu(job, tmp_path):
+    """spacetime=dyst reads dyst_file (sim-org/param.opts:6); a missing or
+    unreadable file is refused by init before any device is touched."""
+    assert job.conf("st=dyst") == 0 and job.conf("flow=thermal") == 0
+    assert job.desc().spacetime == api.ST_NUMERICAL
+    assert job.conf("data=" + str(tmp_path / "absent.h5")) == 0
+    assert job.init() == api.ENOTFOUND
+    bad = tmp_path / "uniform.h5"
+    n = 5
+    u = np.linspace(-40, 40, n)
+    h5.write_spacetime(str(bad), u, u, u, ["0"], [np.zeros((n, n, n, 51), np.float32)])
+    assert job.conf("data=" + str(bad)) == 0
+    assert job.init() == api.EINVAL  # not on the fisheye map interp.cl assumes
+
+
+@pytest.mark.gpu
+def test_cli_dyst_from_hdf5_file(tmp_path):
+    """`gray st=dyst data=file.h5` end to end: a two-snapshot boosted-KS file
+    written in the reference's layout, read by the job, streamed through the
+    snapshot series; every dump equals the oracle's trace on the same grid
+    (reference semantics, in-box camera), and the /rays files hold it too."""
+    n, box, t1, t2 = 20, 40.0, -10.0, 0.0
+    lv = [O.boosted_ks_grid(n, -box, box, t, a=0.7, v=0.3, axis=1) for t in (t1, t2)]
+    xs = O.fisheye_nodes(-box, box, n).astype(np.float32)
+    path = str(tmp_path / "data.h5")
+    h5.write_spacetime(path, xs, xs, xs, ["-10", "0"], [a.astype(np.float32) for a in lv])
+    args = ["st=dyst", "data=" + path, "a=0", "r=30", "i=50", "j=20", "w=30", "h=30",
+            "W=8", "H=6", "dt=-2", "N=3", "n=100", "p=8", "out=" + str(tmp_path / "%04d.raw"),
+            "ray=" + str(tmp_path / "ray%04d.h5")]
+    res = subprocess.run([CLI] + args, capture_output=True, text=True, timeout=300, cwd=tmp_path)
+    assert res.returncode == 0, res.stdout + res.stderr
+    assert "2 snapshot(s)" in res.stdout and "3: -4.0 -> -6.0: DONE" in res.stdout
+    og = O.Grid([a.astype(np.float32) for a in lv], [t1, -box, -box, -box, t2, box, box, box])
+    cfg = dict(a_spin=0.0, r_obs=30.0, i_obs=50.0, j_obs=20.0, w_img=30.0, h_img=30.0,
+               n_width=8, n_height=6, dt_dump=-2.0, n_sub=100)
+    for i in range(1, 4):
+        data, _ = read_raw(str(tmp_path / ("%04d.raw" % i)))
+        ref, _, _ = O.dyst_trace(dict(cfg, n_dump=i), og, np.arange(48))
+        fin = np.all(np.isfinite(ref), axis=1)
+        assert np.array_equal(np.all(np.isfinite(data), axis=1), fin)
+        err = np.max(np.abs(data[fin] - ref[fin]) / np.abs(ref[fin]).max(axis=1, keepdims=True))
+        assert err <= 1e-10, (i, err)
+        with h5.File(str(tmp_path / ("ray%04d.h5" % i))) as f:
+            assert np.array_equal(f.read("rays").reshape(48, 8), data, equal_nan=True)
