@@ -993,7 +993,8 @@ cudaError_t measure_peak(int precision, int sms, cudaStream_t st, double *flops)
 extern "C" int
 gray_measure_peak(gray_ctx *c, int precision, double *flops)
 {
-	if(!c || !flops || (precision != GRAY_PREC_FP64 && precision != GRAY_PREC_MIXED))
+	if(!c || !flops || (precision != GRAY_PREC_FP64 && precision != GRAY_PREC_MIXED &&
+	                    precision != GRAY_PEAK_L1_GATHER))
 		return GRAY_EINVAL;
 	CK(cudaSetDevice(c->device));
 	CK(measure_peak(precision, c->sms, c->stream, flops));

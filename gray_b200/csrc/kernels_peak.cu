@@ -72,12 +72,77 @@ fma64_kernel(double *out, int iters, double a, double b)
 		out[0] = s;
 }
 
+/* L1 gather bandwidth: every lane of a warp loads 32 bytes (one
+ * ld.global.nc.v8.f32, the numerical kernel's grid-row load) from a
+ * different 128-byte line of a 16 KiB window that stays resident in L1,
+ * the access pattern of the corner gathers (each ray its own cell) with no
+ * misses.  Each load feeds an add chain so that it is not dead. */
+__global__ void __launch_bounds__(256)
+l1_gather_kernel(const float *__restrict__ buf, float *out, int iters)
+{
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+	for(int i = 0; i < iters; ++i) {
+		/* 128 lines of 4 sectors: the 32 lanes hit 32 distinct lines */
+		const int line = (lane + 33 * i + 5 * warp) & 127;
+		const float *src = buf + (line * 4 + (i & 3)) * 8;
+		float v[8];
+		asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+		             : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]),
+		               "=f"(v[6]), "=f"(v[7])
+		             : "l"(src));
+		acc[i & 3] += (v[0] + v[1]) + (v[2] + v[3]) + ((v[4] + v[5]) + (v[6] + v[7]));
+	}
+	const float s = acc[0] + acc[1] + acc[2] + acc[3];
+	if(s == 12345.678f)
+		out[0] = s;
+}
+
+/* Bytes/s of the best of 5 timed launches of the L1 gather pattern. */
+cudaError_t
+measure_l1(int sms, cudaStream_t st, double *bps)
+{
+	const int block = 256, iters = 1 << 15, reps = 5;
+	const unsigned grid = (unsigned)sms * 8;
+	const size_t window = 16384; /* 128 lines x 128 bytes */
+	float *buf = nullptr;
+	cudaEvent_t e0, e1;
+	cudaError_t e = cudaMalloc((void **)&buf, window + 64);
+	if(e != cudaSuccess)
+		return e;
+	e = cudaMemsetAsync(buf, 0, window + 64, st);
+	cudaEventCreate(&e0);
+	cudaEventCreate(&e1);
+	double best = 0.0;
+	for(int r = 0; r < reps + 1 && e == cudaSuccess; ++r) {
+		cudaEventRecord(e0, st);
+		l1_gather_kernel<<<grid, block, 0, st>>>(buf, buf + window / sizeof(float), iters);
+		cudaEventRecord(e1, st);
+		e = cudaEventSynchronize(e1);
+		if(e != cudaSuccess)
+			break;
+		float ms = 0.0f;
+		cudaEventElapsedTime(&ms, e0, e1);
+		const double bytes = (double)grid * block * iters * 32.0;
+		if(r > 0 && ms > 0.0f && bytes / (ms * 1e-3) > best)
+			best = bytes / (ms * 1e-3);
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	cudaFree(buf);
+	*bps = best;
+	return e;
+}
+
 } /* namespace */
 
-/* Returns FLOP/s (FMA = 2 FLOP) of the best of `reps` timed launches. */
+/* Returns FLOP/s (FMA = 2 FLOP) of the best of `reps` timed launches; with
+ * GRAY_PEAK_L1_GATHER, the bytes/s of the L1 gather pattern. */
 cudaError_t
 measure_peak(int precision, int sms, cudaStream_t st, double *flops)
 {
+	if(precision == GRAY_PEAK_L1_GATHER)
+		return measure_l1(sms, st, flops);
 	const int block = 256, iters = 1 << 14, reps = 5;
 	const unsigned grid = (unsigned)sms * 8;
 	void *buf = nullptr;

@@ -33,3 +33,29 @@ def test_reference_arm_other_ranks_exit_quietly():
             env={"RANK": "1", "LOCAL_RANK": "1", "WORLD_SIZE": "2"})
     assert p.returncode == 0, p.stderr[-2000:]
     assert p.stdout.strip() == ""
+
+
+def test_cpu_legs_time_one_fixed_sample():
+    """The GPU arm's cpu_baseline leg and the reference arm time the same
+    fixed ray sample (the same indices, every dump interval) split the same
+    way, so their rates differ only by timing noise; the FP32 build of the
+    restatement is reported beside the FP64 one with its image error."""
+    import argparse
+    import sys
+    sys.path.insert(0, ROOT)
+    import bench
+    from gray_b200 import configs
+    cfg = configs.scaled(configs.TORUS_RT_1024, 32)
+    rays = bench.cpu_sample(32 * 32, 64)
+    assert len(set(rays.tolist())) == 64 and rays.max() < 32 * 32
+    assert list(rays) == list(bench.cpu_sample(32 * 32, 64))  # fixed: the same every run
+    args = argparse.Namespace(cpu_rays=64, steps=3, workload="torus_rt_1024")
+    res = bench.analytic_cpu(cfg, args)
+    assert res["kind"] == "port" and res["precision"] == "fp64" and res["value"] > 0
+    assert "64 rays" in res["sample"] and "in 3 parts" in res["sample"]
+    assert res["fp32"]["value"] > 0 and res["fp32"]["image_rel_l2_err_vs_fp64"] > 0
+    p = run(["--impl", "reference", "--steps", "3", "--warmup", "3", "--cpu-rays", "64",
+             "--side", "32"])
+    assert p.returncode == 0, p.stderr[-2000:]
+    line = json.loads(p.stdout.strip().splitlines()[-1])
+    assert "64 rays" in line["cpu_baseline"]["sample"] and "in 3 parts" in line["cpu_baseline"]["sample"]

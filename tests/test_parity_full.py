@@ -82,6 +82,17 @@ def test_torus_1024_mixed_image_error(torus):
     assert max(errs) <= TOL_MIXED
     assert pos <= TOL_MIXED
     assert abs(nmx - n64) <= 1e-3 * n64
+    # rays that end at the horizon (the stop rule eps < 0.01 fired): every
+    # one of them passed within 0.1 M of r_+, where the RHS radius root is
+    # FP32 and the stop and step rules use the FP64 island
+    a = cfg["a_spin"]
+    x, y, z = s64[1], s64[2], s64[3]
+    kk = 0.5 * (x * x + y * y + z * z - a * a)
+    r = np.sqrt(np.sqrt(kk * kk + a * a * z * z) + kk)
+    near = r < 1.0 + np.sqrt(1.0 - a * a) + 0.1
+    cap = image_err(smx[1:4, near], s64[1:4, near])
+    print("rays ending within 0.1 M of r_+: %d, end position rel L2 %.3e" % (near.sum(), cap))
+    assert cap <= TOL_MIXED
     # null constraint relative to |u|^2 (captured rays end with large u)
     norm = np.sum(smx[4:8] ** 2, axis=0)
     assert np.max(np.abs(imx) / norm) < 1e-5
