@@ -53,7 +53,7 @@ METRIC = "ray-steps/s"
 
 # DRAM bytes (read + write) of one full-size launch of the dominant kernel,
 # from one-pass ncu captures (dram__bytes_read.sum + dram__bytes_write.sum).
-TRAFFIC = {"torus_rt_1024": 145832704 + 116188928,
+TRAFFIC = {"torus_rt_1024": 151332352 + 143093504,
            "numerical_128": 500394240 + 17862656}
 # Host-to-device bytes of one render through the C ABI: the render's table
 # entry (sizeof(MixedRender) in gray_b200/csrc/mixed_table.h); the camera
@@ -692,8 +692,8 @@ def numerical_arm(args, cfg, rank, local_rank, world, dist):
     traffic = None if args.side else TRAFFIC.get(args.workload)
     roofline = {"bound": "l1", "achieved": achieved, "peak": l1, "unit": "GB/s",
                 "frac": achieved / l1, "traffic": traffic,
-                "peak_source": "L1 gather microbenchmark in this run (32-byte loads, one "
-                               "128-byte line per lane, all hits)",
+                "peak_source": "L1 load microbenchmark in this run (32-byte loads, all hits, "
+                               "full lines)",
                 "bytes_per_gather_step": per_step, "levels_read": levels,
                 "hbm": {"dram_bytes_per_launch": traffic, "peak": hbm, "peak_source": hbm_src,
                         "frac": (traffic / (ker / args.steps) / 1e9 / hbm) if traffic else None},

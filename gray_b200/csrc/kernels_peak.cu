@@ -72,20 +72,21 @@ fma64_kernel(double *out, int iters, double a, double b)
 		out[0] = s;
 }
 
-/* L1 gather bandwidth: every lane of a warp loads 32 bytes (one
- * ld.global.nc.v8.f32, the numerical kernel's grid-row load) from a
- * different 128-byte line of a 16 KiB window that stays resident in L1,
- * the access pattern of the corner gathers (each ray its own cell) with no
- * misses.  Each load feeds an add chain so that it is not dead. */
+/* L1 load bandwidth with the numerical kernel's load instruction: 32-byte
+ * loads (ld.global.nc.v8.f32) from a 16 KiB window that stays resident in
+ * L1, a warp's 32 lanes reading 32 consecutive rows (1 KiB, fully used
+ * lines), so that the L1 data path, not its tag lookups, is the limit: the
+ * ceiling of any gather that hits in L1.  Each load feeds an add chain so
+ * that it is not dead. */
 __global__ void __launch_bounds__(256)
 l1_gather_kernel(const float *__restrict__ buf, float *out, int iters)
 {
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 	for(int i = 0; i < iters; ++i) {
-		/* 128 lines of 4 sectors: the 32 lanes hit 32 distinct lines */
-		const int line = (lane + 33 * i + 5 * warp) & 127;
-		const float *src = buf + (line * 4 + (i & 3)) * 8;
+		/* 512 rows of 32 bytes; warp w reads rows 32 (i + w) .. + 31 */
+		const int row = (32 * (i + warp) + lane) & 511;
+		const float *src = buf + row * 8;
 		float v[8];
 		asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
 		             : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]),
@@ -98,7 +99,7 @@ l1_gather_kernel(const float *__restrict__ buf, float *out, int iters)
 		out[0] = s;
 }
 
-/* Bytes/s of the best of 5 timed launches of the L1 gather pattern. */
+/* Bytes/s of the best of 5 timed launches of the L1 load pattern. */
 cudaError_t
 measure_l1(int sms, cudaStream_t st, double *bps)
 {
@@ -137,7 +138,7 @@ measure_l1(int sms, cudaStream_t st, double *bps)
 } /* namespace */
 
 /* Returns FLOP/s (FMA = 2 FLOP) of the best of `reps` timed launches; with
- * GRAY_PEAK_L1_GATHER, the bytes/s of the L1 gather pattern. */
+ * GRAY_PEAK_L1_GATHER, the L1 load bandwidth in bytes/s. */
 cudaError_t
 measure_peak(int precision, int sms, cudaStream_t st, double *flops)
 {

@@ -415,9 +415,9 @@ int gray_run_mixed_noalloc(int device, const gray_render_desc *descs, int n_rend
 /* CUDA-core FMA-loop peak of the context's device in FLOP/s (FMA = 2):
  * the roofline denominator of the geodesic kernels.  precision selects
  * FP64 or FP32 (best of scalar and packed f32x2 FMA).  With
- * GRAY_PEAK_L1_GATHER it is instead the L1 bandwidth in bytes/s of the
- * numerical kernel's gather pattern (every lane a 32-byte load from its own
- * 128-byte line, all hits): the roofline denominator of the grid gathers. */
+ * GRAY_PEAK_L1_GATHER it is instead the L1 load bandwidth in bytes/s with
+ * the numerical kernel's 32-byte loads, all hits and fully used lines: the
+ * ceiling of the grid gathers, which hit L1 for 95% of their sectors. */
 #define GRAY_PEAK_L1_GATHER 2
 int gray_measure_peak(gray_ctx *ctx, int precision, double *flops);
 
