@@ -255,6 +255,11 @@ def getrr(a, q):
     return lib().orc_getrr(a, _p(q))
 
 
+def geteps(a, q):
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    return lib().orc_geteps(a, _p(q))
+
+
 def getdt(cfg, q, dt):
     d = make_desc(cfg)
     q = np.ascontiguousarray(q, dtype=np.float64)
@@ -428,3 +433,102 @@ def coords(a, s, system="bl", r_match=10.0, as_written=False):
         L.orc_getBL(a, r_match, _p(q), w, _p(x))
         L.orc_getBLu(a, _p(q), _p(u), w, _p(v))
     return np.r_[x, v]
+
+
+# ---------------------------------------------------------------------------
+# The reference's own kernel sources built for the CPU (oracle/_ref, see
+# oracle/ref_shim): the pins of the restatement above.  Present only where
+# the reference tree was available at build time.
+
+REF_DIR = os.path.join(HERE, "_ref")
+_ref = {}
+
+
+def ref_available():
+    return all(os.path.exists(os.path.join(REF_DIR, f))
+               for f in ("libref_ks.so", "libref_dyst.so"))
+
+
+def _reflib(name):
+    if name not in _ref:
+        _ref[name] = ctypes.CDLL(os.path.join(REF_DIR, name))
+    return _ref[name]
+
+
+class RefKsDesc(ctypes.Structure):
+    _fields_ = ([(n, ctypes.c_double) for n in ("a_spin", "w_img", "h_img", "r_obs", "i_obs",
+                                                "j_obs")] +
+                [("w_rays", ctypes.c_int64), ("h_rays", ctypes.c_int64),
+                 ("t_init", ctypes.c_double), ("dt_dump", ctypes.c_double),
+                 ("n_sub", ctypes.c_int64), ("n_dump", ctypes.c_int64)])
+
+
+class RefDystDesc(ctypes.Structure):
+    _fields_ = ([(n, ctypes.c_double) for n in ("w_img", "h_img", "r_obs", "i_obs", "j_obs")] +
+                [("w_rays", ctypes.c_int64), ("h_rays", ctypes.c_int64),
+                 ("t_init", ctypes.c_double), ("dt_dump", ctypes.c_double),
+                 ("n_sub", ctypes.c_int64), ("n_dump", ctypes.c_int64),
+                 ("nu", ctypes.c_double), ("m_adm", ctypes.c_double),
+                 ("box", ctypes.c_double * 8), ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+                 ("nz", ctypes.c_int)])
+
+
+def ref_ks_rhs(a, s):
+    """KS.cl gr_rhs() itself at state s[8]."""
+    L = _reflib("libref_ks.so")
+    s = np.ascontiguousarray(s, dtype=np.float64)
+    ds = np.zeros(8)
+    L.ref_ks_rhs(ctypes.c_double(a), _p(s), _p(ds))
+    return ds
+
+
+def ref_ks_func(name, a, q, u=None):
+    """KS.cl getrr / geteps (scalar) or down (4-vector) itself."""
+    L = _reflib("libref_ks.so")
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    if name == "down":
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        k = np.zeros(4)
+        L.ref_ks_down(ctypes.c_double(a), _p(q), _p(u), _p(k))
+        return k
+    f = getattr(L, "ref_ks_" + name)
+    f.restype = ctypes.c_double
+    return f(ctypes.c_double(a), _p(q))
+
+
+def ref_ks_trace(cfg, rays):
+    """icond_drv + evolve_drv of the reference's analytic program over the
+    listed rays: (states [n, 8], info [n])."""
+    L = _reflib("libref_ks.so")
+    d = RefKsDesc(cfg.get("a_spin", 0.0), cfg.get("w_img", 64.0), cfg.get("h_img", 64.0),
+                  cfg.get("r_obs", 1024.0), cfg.get("i_obs", 60.0), cfg.get("j_obs", 0.0),
+                  cfg["n_width"], cfg["n_height"], cfg.get("t_init", 0.0),
+                  cfg.get("dt_dump", -32.0), cfg.get("n_sub", 1024), cfg.get("n_dump", 64))
+    rays = np.ascontiguousarray(rays, dtype=np.int64)
+    out, info = np.zeros((rays.size, 8)), np.zeros(rays.size)
+    if L.ref_ks_trace(ctypes.byref(d), _pi(rays), ctypes.c_int64(rays.size), _p(out),
+                      _p(info)) != 0:
+        raise ValueError("ray index outside the image")
+    return out, info
+
+
+def ref_dyst_trace(cfg, levels, box, rays):
+    """icond_drv + evolve_drv of the reference's numerical-spacetime program
+    with one frequency of thermal transfer (flow.cl's template flow, rt.cl's
+    emissivities): (states [n, 10], info [n]).  levels are two [nz, ny, nx,
+    51] float32 arrays at box[0] and box[4]."""
+    L = _reflib("libref_dyst.so")
+    lv = [np.ascontiguousarray(a, dtype=np.float32) for a in levels]
+    nz, ny, nx, _ = lv[0].shape
+    d = RefDystDesc(cfg.get("w_img", 64.0), cfg.get("h_img", 64.0), cfg.get("r_obs", 1024.0),
+                    cfg.get("i_obs", 60.0), cfg.get("j_obs", 0.0), cfg["n_width"],
+                    cfg["n_height"], cfg.get("t_init", 0.0), cfg.get("dt_dump", -32.0),
+                    cfg.get("n_sub", 1024), cfg.get("n_dump", 64), cfg["nu"][0],
+                    cfg.get("m_adm", 4.3e6), (ctypes.c_double * 8)(*box), nx, ny, nz)
+    rays = np.ascontiguousarray(rays, dtype=np.int64)
+    out, info = np.zeros((rays.size, 10)), np.zeros(rays.size)
+    if L.ref_dyst_trace(ctypes.byref(d), ctypes.c_void_p(lv[0].ctypes.data),
+                        ctypes.c_void_p(lv[1].ctypes.data), _pi(rays),
+                        ctypes.c_int64(rays.size), _p(out), _p(info)) != 0:
+        raise ValueError("ray index outside the image")
+    return out, info
