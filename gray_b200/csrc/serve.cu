@@ -55,6 +55,7 @@ struct Request {
 	double *d_data = nullptr, *d_info = nullptr;
 	size_t bytes = 0;
 	int next_dump = 0;
+	int window = 0;  /* dump intervals of the current iteration */
 	std::atomic<bool> cancel{false}; /* set by gray_serve_cancel, read by the scheduler */
 	std::vector<double> h_data, h_info;
 
@@ -141,8 +142,20 @@ iterate(Server *S, std::vector<Request *> &fresh)
 	if(S->inflight.empty())
 		return GRAY_OK;
 
-	/* 2. one table per group, entries with the next window of dumps */
+	/* 2. one table per group, entries with the next window of dumps.  The
+	 * largest admitted render advances dumps_per_iter intervals; a smaller
+	 * one advances as many intervals as the same ray-intervals of work
+	 * allow (at most the ones it has left), so it finishes in fewer
+	 * iterations while the iteration's length stays set by the largest */
 	const int dpi = S->cfg.dumps_per_iter;
+	long long max_rays = 1;
+	for(Request *r : S->inflight)
+		max_rays = std::max(max_rays, r->p.n_rays);
+	for(Request *r : S->inflight) {
+		const double w = (double)dpi * (double)max_rays / (double)std::max(1LL, r->p.n_rays);
+		const int left = (int)r->desc.n_dump - r->next_dump;
+		r->window = std::max(1, std::min(left, w < (double)left ? std::max(dpi, (int)w) : left));
+	}
 	int count[GROUPS] = {0}, start[GROUPS];
 	for(Request *r : S->inflight)
 		count[r->group()]++;
@@ -160,7 +173,7 @@ iterate(Server *S, std::vector<Request *> &fresh)
 		fill_mixed_render(r->p, r->d_data, r->d_info, r->desc.t_init, r->desc.dt_dump,
 		                  (long long)r->desc.n_dump, (long long)r->desc.n_sub, &m);
 		m.dump_begin = r->next_dump;
-		m.dump_end = std::min(r->next_dump + dpi, (int)r->desc.n_dump);
+		m.dump_end = r->next_dump + r->window;
 		S->h_pre[k] = total[g];
 		total[g] += (unsigned long long)r->p.n_rays;
 	}
@@ -210,7 +223,7 @@ iterate(Server *S, std::vector<Request *> &fresh)
 	/* 3. advance windows, retire finished renders */
 	std::vector<Request *> keep, done;
 	for(Request *r : S->inflight) {
-		r->next_dump = std::min(r->next_dump + dpi, (int)r->desc.n_dump);
+		r->next_dump += r->window;
 		if(r->next_dump >= (int)r->desc.n_dump || r->cancel)
 			done.push_back(r);
 		else

@@ -250,9 +250,12 @@ int gray_get_plan(const gray_ctx *ctx, gray_launch_plan *plan);
 
 /* A scheduler thread owned by the context admits submitted renders as HBM
  * (the configured budget) and table slots free up, and advances every
- * admitted render by dumps_per_iter dump intervals per iteration: one
+ * admitted render by a window of dump intervals per iteration: one
  * persistent launch per kind (analytic by n_freq, numerical), so renders
- * that arrived while others run share the device with them.  Finished
+ * that arrived while others run share the device with them.  The largest
+ * admitted render advances dumps_per_iter intervals; a render with fewer
+ * rays advances as many more as keep its work (rays x intervals) at the
+ * largest one's, so small renders finish within an iteration or two.  Finished
  * renders are copied to host memory and their device state is freed.  Only
  * mixed-precision renders are served; numerical ones use the context's
  * grid, which must be loaded before gray_serve_start.  While the server
