@@ -154,7 +154,8 @@ iterate(Server *S, std::vector<Request *> &fresh)
 	for(Request *r : S->inflight) {
 		const double w = (double)dpi * (double)max_rays / (double)std::max(1LL, r->p.n_rays);
 		const int left = (int)r->desc.n_dump - r->next_dump;
-		r->window = std::max(1, std::min(left, w < (double)left ? std::max(dpi, (int)w) : left));
+		/* left = 0 (no dump intervals): an empty window, the render is done */
+		r->window = left <= 0 ? 0 : std::min(left, w < (double)left ? std::max(dpi, (int)w) : left);
 	}
 	int count[GROUPS] = {0}, start[GROUPS];
 	for(Request *r : S->inflight)

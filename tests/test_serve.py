@@ -156,3 +156,30 @@ def test_stop_without_drain_drops_pending(ctx):
     ids = [ctx.submit(dict(configs.scaled(configs.TORUS_RT_1024, 48))) for _ in range(3)]
     assert ctx.serve_stop(drain=False) == api.OK
     del ids
+
+
+def test_windows_sized_by_work_and_empty_requests(ctx):
+    """A large render and several small ones together: the small ones get
+    windows of the large one's work and finish in an iteration or two, with
+    the same results as alone; a request with no dump intervals returns its
+    camera state."""
+    big = dict(configs.scaled(configs.TORUS_RT_1024, 96), n_dump=24)
+    small = [dict(configs.scaled(configs.TORUS_RT_1024, 8), n_dump=24, i_obs=float(10 + 20 * k))
+             for k in range(3)]
+    empty = dict(configs.scaled(configs.TORUS_RT_1024, 8), n_dump=0)
+    reqs = [big] + small + [empty]
+    ref = [alone(ctx, c) for c in reqs]
+    ctx.serve_start(max_inflight=16, dumps_per_iter=2)
+    try:
+        ids = [ctx.submit(c) for c in reqs]
+        assert all(s == api.REQ_DONE for s in wait(ctx, ids))
+        stats, _ = ctx.serve_stats()
+        for rid, c, (d, info) in zip(ids, reqs, ref):
+            got, ginfo = ctx.result(rid, 8 + 2 * len(c["nu"]), c["n_width"] * c["n_height"])
+            scale = np.maximum(np.abs(d), 1e-300).max(axis=1, keepdims=True)
+            assert np.max(np.abs(got - d) / scale) <= 1e-6
+        # the large render needs 12 iterations of 2 intervals; the small ones
+        # ride along with windows of 24 and add none
+        assert stats.iterations <= 14
+    finally:
+        ctx.serve_stop()
