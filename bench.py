@@ -924,8 +924,8 @@ def extra_workloads(args, rank, local_rank, world, dist):
     """The other single-GPU workloads, shortened, in the default run's line:
     survey_256 (the whole 256-render batch, one timed step, the FP64
     comparison on its first 8 renders alone), numerical_128 (3 timed
-    renders) and serve_mix (16 requests per rate, rates 0.5 to 3 per second
-    until the slowdown rule fails).  Their measurement rules are those of
+    renders) and serve_mix (16 requests per rate, rates 0.5, 1, 1.5, 2, 3
+    per second until the slowdown rule fails).  Their measurement rules are those of
     their own bench lines."""
     import copy
     out = {}
@@ -945,7 +945,7 @@ def extra_workloads(args, rank, local_rank, world, dist):
         out["numerical_128"] = dict({k: n[k] for k in keep + ("cpu_baseline",) if k in n},
                                     config=n["config"])
     a = copy.copy(args)
-    a.requests, a.rates, a.workload = 16, "0.5,0.75,1,1.5,2,3", "serve_mix"
+    a.requests, a.rates, a.workload = 16, "0.5,1,1.5,2,3", "serve_mix"
     v = serve_arm(a, rank, local_rank, world, dist)
     if v is not None:
         out["serve_mix"] = {k: v[k] for k in ("value", "unit", "latency", "sweep", "error_vs_fp64",
