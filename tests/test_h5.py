@@ -1,8 +1,13 @@
 """GRay2's HDF5 files without libhdf5 (gray_b200/host/gray_h5.c).
 
-No HDF5 implementation exists on either machine to cross-check against
-(no libhdf5, no h5py), so parity with libhdf5 is unpinned.  These tests
-check instead that:
+No HDF5 library exists on either machine to cross-check against (no
+libhdf5, no h5py).  One file written by libhdf5 does: scipy ships a MATLAB
+v7.3 test file, which is a classic-format HDF5 file behind a 512-byte user
+block.  The reader is pinned to it; the writer is not pinned to libhdf5.
+These tests check that:
+ - the reader reads that libhdf5 file (user block and base address,
+   layout message v2, fill-value message v1, attribute, modification-time
+   and NIL messages skipped) to the exact values MATLAB stored;
  - what the writer writes reads back exactly (spacetime files in the
    README.md:40-60 / io.c:356-428 layout, /rays files of sim/gray.c:170-176);
  - the written bytes carry the published HDF5 format fields, parsed here by
@@ -256,3 +261,35 @@ def test_non_fisheye_coordinates_are_refused(tmp_path):
         h5.Spacetime(path)
     assert e.value.status == h5.EFORMAT
     assert os.path.exists(path)
+
+
+# ------------------------------------------------------- a file libhdf5 wrote
+
+def libhdf5_file():
+    """scipy's MATLAB 7.4 test file saved in the v7.3 (HDF5) format: one
+    9 x 1 double dataset, 0:pi/4:2*pi, with a MATLAB_class attribute."""
+    scipy = pytest.importorskip("scipy")
+    path = os.path.join(os.path.dirname(scipy.__file__), "io", "matlab", "tests", "data",
+                        "testhdf5_7.4_GLNX86.mat")
+    if not os.path.exists(path):
+        pytest.skip("scipy's MATLAB test data is not installed")
+    return path
+
+
+def test_reads_a_file_written_by_libhdf5():
+    path = libhdf5_file()
+    data = open(path, "rb").read()
+    assert data[512:520] == b"\x89HDF\r\n\x1a\n"  # behind the MAT user block
+    with h5.File(path) as f:
+        assert f.members("/") == ["testdouble"]
+        dims, elem = f.info("testdouble")
+        assert dims == (9, 1) and elem == 8
+        v = f.read("/testdouble")
+        assert v.dtype == np.float64 and v.shape == (9, 1)
+        assert np.array_equal(v.ravel(), np.arange(9) * (np.pi / 4))
+        with pytest.raises(h5.H5Error) as e:
+            f.read("testsingle")
+        assert e.value.status == h5.ENOTFOUND
+    with pytest.raises(h5.H5Error) as e:  # no grid group: not a spacetime file
+        h5.Spacetime(path)
+    assert e.value.status in (h5.ENOTFOUND, h5.EFORMAT)
