@@ -56,9 +56,11 @@ METRIC = "ray-steps/s"
 TRAFFIC = {"torus_rt_1024": 151332352 + 143093504,
            "numerical_128": 500394240 + 17862656}
 # Host-to-device bytes of one render through the C ABI: the render's table
-# entry (sizeof(MixedRender) in gray_b200/csrc/mixed_table.h); the camera
-# initial conditions are generated on the device.
-H2D_BYTES_PER_RENDER = 392
+# entry (sizeof(MixedRender) in gray_b200/csrc/mixed_table.h), which the
+# analytic kernel's one-render launch also carries as its kernel parameter;
+# the camera initial conditions are generated on the device.
+H2D_BYTES_PER_RENDER = 440
+H2D_BYTES_ANALYTIC = 2 * H2D_BYTES_PER_RENDER
 
 
 def parse():
@@ -448,7 +450,7 @@ def ours_arm(args, cfg, rank, local_rank, world, dist):
     barrier(torch, dist)
     e2e_t = max_over_ranks(torch, dist, e2e_t)
     e2e = {"value": job_steps * args.e2e_steps / e2e_t, "unit": "ray-steps/s",
-           "h2d_bytes_per_step": H2D_BYTES_PER_RENDER,
+           "h2d_bytes_per_step": H2D_BYTES_ANALYTIC,
            "d2h_bytes_per_step": int(host.nbytes + hinfo.nbytes)}
     if world > 1:
         e2e["bytes_note"] = "per rank"

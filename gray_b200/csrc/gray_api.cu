@@ -529,7 +529,7 @@ run_mixed(gray_ctx *c, Render *r, double t_init, double dt_dump, long long n_dum
 		CK(launch_dyst_mixed_table(T, c->grid->gp, r->p.n_freq, r->d_queue, r->d_steps,
 		                           c->stream, c->mixed, r->d_steps + 1));
 	} else {
-		CK(launch_mixed_table(T, r->p.n_freq, r->d_queue, r->d_steps, c->stream, c->mixed));
+		CK(launch_mixed_table(T, r->p.n_freq, r->d_queue, r->d_steps, c->stream, c->mixed, &m));
 	}
 	return GRAY_OK;
 }

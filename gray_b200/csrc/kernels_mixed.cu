@@ -32,6 +32,7 @@
  *    loaded), not re-read from the table every RHS.
  */
 #include <climits>
+#include <cstring>
 
 #include "gray_internal.h"
 #include "logk2_table.h"
@@ -195,24 +196,54 @@ tau_ratio(const MixedRender &c, int i)
 	return q * q;
 }
 
-template <typename V, int NF>
+/* The render's constants into lane k of rc.  With UNI (a one-render
+ * launch) only the per-ray part is held in registers: k_t and the
+ * frequencies' optical-depth offsets; uni_rc() supplies the rest from the
+ * kernel parameter at each step. */
+template <typename V, int NF, bool UNI>
 __device__ __forceinline__ void
 load_rc(RC<V, NF> &rc, int k, const MixedRender &c, double kt, const double *tau0)
 {
-	setl(rc.a, k, c.a);
-	setl(rc.aa, k, c.aa);
-	setl(rc.risco, k, c.risco);
-	/* the density scale, zero without the torus flow */
-	setl(rc.n0t, k, c.flow == GRAY_FLOW_TORUS ? c.n0_rp15 : 0.0f);
-	setl(rc.ihr2, k, c.ihr2_log2e);
-	setl(rc.kap0, k, NF > 0 ? c.kappa * c.nuinv2[0] : 0.0f);
+	if constexpr(!UNI) {
+		setl(rc.a, k, c.a);
+		setl(rc.aa, k, c.aa);
+		setl(rc.risco, k, c.risco);
+		setl(rc.n0t, k, c.n0t);
+		setl(rc.ihr2, k, c.ihr2_log2e);
+		setl(rc.kap0, k, c.kap0);
+	}
 	setl(rc.kt, k, (float)kt);
 #pragma unroll
 	for(int i = 0; i < NF; ++i) {
 		const double q = tau_ratio(c, i);
 		const double off = tau0[i] - q * tau0[0];
 		setl(rc.lgnu[i], k, log2f(c.nupow[i]) - (float)(1.4426950408889634 * off));
-		setl(rc.tcoef[i], k, (float)(-1.4426950408889634 * q));
+		if constexpr(!UNI)
+			setl(rc.tcoef[i], k, c.tcoef[i]);
+	}
+}
+
+/* The constants of a step: rc as loaded, or with UNI the render-wide ones
+ * taken from the kernel parameter, which the compiler reads as constant
+ * bank operands instead of keeping them live in registers. */
+template <typename V, int NF, bool UNI>
+__device__ __forceinline__ RC<V, NF>
+step_rc(const RC<V, NF> &rc, const MixedRender &R)
+{
+	if constexpr(!UNI) {
+		return rc;
+	} else {
+		RC<V, NF> o = rc;
+		o.a = bc<V>(R.a);
+		o.aa = bc<V>(R.aa);
+		o.risco = bc<V>(R.risco);
+		o.n0t = bc<V>(R.n0t);
+		o.ihr2 = bc<V>(R.ihr2_log2e);
+		o.kap0 = bc<V>(R.kap0);
+#pragma unroll
+		for(int i = 0; i < NF; ++i)
+			o.tcoef[i] = bc<V>(R.tcoef[i]);
+		return o;
 	}
 }
 
@@ -411,20 +442,36 @@ struct Slot {
 };
 
 /* Per-dump constants, computed in FP64 exactly like the host loop of
- * sim-org/gray.c:251-252 and driver.cl:93. */
+ * sim-org/gray.c:251-252 and driver.cl:93; n is the render's ticks per
+ * dump interval. */
 __device__ __forceinline__ void
-start_dump(Slot &S)
+start_dump(Slot &S, const MixedRender &c, int n)
 {
-	const MixedRender &c = *S.c;
 	double t      = c.t_init + (double)S.dump * c.dt_dump;
 	double target = c.t_init + (double)(S.dump + 1) * c.dt_dump;
 	double dt     = target - t;
 	double dts    = dt / (double)c.n_sub;
-	S.dh_cap = (int)(dts / dt * (double)S.n);
-	S.cdt    = (float)((double)S.n / fabs(dt));
-	S.dtn    = (float)(dt / (double)S.n);
+	S.dh_cap = (int)(dts / dt * (double)n);
+	S.cdt    = (float)((double)n / fabs(dt));
+	S.dtn    = (float)(dt / (double)n);
 	S.h      = 0;
 }
+
+/* A slot's render-wide values: from the slot (loaded with the ray) or, with
+ * UNI, from the kernel parameter. */
+template <bool UNI>
+struct SlotView {
+	const Slot &S;
+	const MixedRender &R;
+	__device__ __forceinline__ const MixedRender &render() const { return UNI ? R : *S.c; }
+	__device__ __forceinline__ int n() const { return UNI ? R.n_ticks : S.n; }
+	__device__ __forceinline__ int dump_end() const { return UNI ? R.dump_end : S.dump_end; }
+	__device__ __forceinline__ float rp() const { return UNI ? R.rp : S.rp; }
+	__device__ __forceinline__ float eps_stop() const { return UNI ? R.eps_stop : S.eps_stop; }
+	__device__ __forceinline__ float cdt_scale() const { return UNI ? R.cdt_scale : S.cdt_scale; }
+	__device__ __forceinline__ double aa_d() const { return UNI ? R.aa_d : S.aa_d; }
+	__device__ __forceinline__ double rp_d() const { return UNI ? R.rp_d : S.rp_d; }
+};
 
 /* Final state to HBM in the reference's layout: x^mu, u^mu (from k_mu in
  * FP64), I_nu, tau_nu (tau_i rebuilt from tau_0) and g(u,u).  The ray's
@@ -470,7 +517,7 @@ store_ray(const MixedRender &c, long long ray, int nf, const float *hi, const fl
 
 template <typename V, int NF>
 __device__ __forceinline__ void
-store_slot(const Slot &S, int k, const V *hi, const V *lo)
+store_slot(const MixedRender &c, const Slot &S, int k, const V *hi, const V *lo)
 {
 	constexpr int NI = Layout<NF>::NI;
 	float h[NI], l[NI];
@@ -479,7 +526,7 @@ store_slot(const Slot &S, int k, const V *hi, const V *lo)
 		h[i] = getl(hi[i], k);
 		l[i] = getl(lo[i], k);
 	}
-	store_ray(*S.c, S.ray, NF, h, l);
+	store_ray(c, S.ray, NF, h, l);
 }
 
 /* Map a global queue index to (render, ray) by binary search over the
@@ -500,27 +547,28 @@ find_render(const MixedTable &T, unsigned long long g)
 
 /* Step size of slot k in ticks (phys.cl:48-64 via driver.cl:93), with the
  * FP64 island near r_+; 0 means the ray stops (captured or NaN). */
-template <typename V>
+template <typename V, bool UNI>
 __device__ __forceinline__ int
-ticks(const Slot &S, int k, const V *hi, const V *lo)
+ticks(const SlotView<UNI> &v, int k, const V *hi, const V *lo)
 {
+	const Slot &S = v.S;
 	float x = getl(hi[1], k), y = getl(hi[2], k), z = getl(hi[3], k);
-	float aa = (float)S.aa_d;
+	float aa = (float)v.aa_d();
 	float zz = z * z;
 	float kk = 0.5f * (fmaf(x, x, fmaf(y, y, zz)) - aa);
 	float rr = sqrt_a(fmaf(kk, kk, aa * zz)) + kk;
-	float eps = sqrt_a(rr) - S.rp;
+	float eps = sqrt_a(rr) - v.rp();
 	if(eps < 1.0f) {
 		double xd = (double)x - (double)getl(lo[1], k);
 		double yd = (double)y - (double)getl(lo[2], k);
 		double zd = (double)z - (double)getl(lo[3], k);
-		eps = (float)(sqrt(getrr_d(S.aa_d, xd, yd, zd)) - S.rp_d);
+		eps = (float)(sqrt(getrr_d(v.aa_d(), xd, yd, zd)) - v.rp_d());
 	}
-	if(!(eps >= S.eps_stop))
+	if(!(eps >= v.eps_stop()))
 		return 0;
-	float want = S.cdt_scale * eps * eps * S.cdt; /* 0.01 eps^2 n / |dt| */
+	float want = v.cdt_scale() * eps * eps * S.cdt; /* 0.01 eps^2 n / |dt| */
 	int dh = want < (float)S.dh_cap ? (int)want : S.dh_cap;
-	return dh < S.n - S.h ? dh : S.n - S.h;
+	return dh < v.n() - S.h ? dh : v.n() - S.h;
 }
 
 /* One RK4 step (RK4.cl:37-47) of size hs on the NI integrated reals with
@@ -598,10 +646,13 @@ rk4_packed(const RC<V, NF> &rc, V *hi, V *lo, V hs)
 	}
 }
 
-template <int NF, typename V, bool ROLLED>
+/* UNI: the table holds one render, passed again by value as R1 (a kernel
+ * parameter); its constants are then not held per ray.  Otherwise R1 is
+ * unused. */
+template <int NF, typename V, bool ROLLED, bool UNI>
 __global__ void __launch_bounds__(Lanes<V>::N == 1 ? 256 : 128, Lanes<V>::N == 1 ? 2 : 1)
-mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
-             unsigned long long *__restrict__ steps)
+mixed_kernel(const MixedTable T, const __grid_constant__ MixedRender R1,
+             unsigned int *__restrict__ queue, unsigned long long *__restrict__ steps)
 {
 	typedef Layout<NF> Y;
 	constexpr int NI = Y::NI;
@@ -644,25 +695,27 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 				exhausted = true;
 				continue;
 			}
-			int rdx = find_render(T, g);
-			const MixedRender &c = T.renders[rdx];
+			const int rdx = UNI ? 0 : find_render(T, g);
+			const MixedRender &c = UNI ? R1 : T.renders[rdx];
 			Slot &s = S[k];
-			s.c = &c;
-			s.ray = (long long)(g - T.prefix[rdx]);
-			s.n = (int)((INT_MAX / c.n_sub) * c.n_sub);
+			s.ray = (long long)(UNI ? g : g - T.prefix[rdx]);
 			s.dump = c.dump_begin;
-			s.dump_end = c.dump_end;
-			s.rp = c.rp;
-			s.eps_stop = c.eps_stop;
-			s.cdt_scale = c.cdt_scale;
-			s.aa_d = c.aa_d;
-			s.rp_d = c.rp_d;
+			if constexpr(!UNI) {
+				s.c = &c;
+				s.n = c.n_ticks;
+				s.dump_end = c.dump_end;
+				s.rp = c.rp;
+				s.eps_stop = c.eps_stop;
+				s.cdt_scale = c.cdt_scale;
+				s.aa_d = c.aa_d;
+				s.rp_d = c.rp_d;
+			}
 			const long long nr = c.n_rays;
 			double s0[8], k0[4], tau0[NF > 0 ? NF : 1];
 #pragma unroll
 			for(int i = 0; i < 8; ++i)
 				s0[i] = c.data[i * nr + s.ray];
-			if(s.dump >= s.dump_end) { /* empty window: state unchanged */
+			if(s.dump >= c.dump_end) { /* empty window: state unchanged */
 				c.info[s.ray] = getuu_d(c.a_d, s0);
 				continue;
 			}
@@ -677,14 +730,14 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 			}
 			if(NF > 0)
 				v[Y::TAU] = tau0[0];
-			load_rc<V, NF>(rc, k, c, k0[0], tau0);
+			load_rc<V, NF, UNI>(rc, k, c, k0[0], tau0);
 #pragma unroll
 			for(int i = 0; i < NI; ++i) {
 				float h = (float)v[i];
 				setl(hi[i], k, h);
 				setl(lo[i], k, (float)((double)h - v[i]));
 			}
-			start_dump(s);
+			start_dump(s, c, c.n_ticks);
 			s.active = true;
 		}
 		bool any = false;
@@ -702,9 +755,10 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 			dh[k] = 0;
 			if(!S[k].active)
 				continue;
-			dh[k] = ticks<V>(S[k], k, hi, lo);
+			const SlotView<UNI> v{S[k], R1};
+			dh[k] = ticks<V, UNI>(v, k, hi, lo);
 			if(dh[k] == 0) {
-				store_slot<V, NF>(S[k], k, hi, lo);
+				store_slot<V, NF>(v.render(), S[k], k, hi, lo);
 				S[k].active = false;
 			} else {
 				step = true;
@@ -748,7 +802,7 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 				hi[i] = tv;
 			}
 		} else if constexpr(L == 1) {
-			rk4_packed<V, NF>(rc, hi, lo, hs);
+			rk4_packed<V, NF>(step_rc<V, NF, UNI>(rc, R1), hi, lo, hs);
 		} else {
 			const V hh = bc<V>(0.5f) * hs;
 			V kk[NI], t[NI], sum[NI];
@@ -788,13 +842,14 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 				continue;
 			++cnt;
 			Slot &s = S[k];
+			const SlotView<UNI> v{s, R1};
 			s.h += dh[k];
-			if(s.h >= s.n) {
-				if(++s.dump >= s.dump_end) {
-					store_slot<V, NF>(s, k, hi, lo);
+			if(s.h >= v.n()) {
+				if(++s.dump >= v.dump_end()) {
+					store_slot<V, NF>(v.render(), s, k, hi, lo);
 					s.active = false;
 				} else {
-					start_dump(s);
+					start_dump(s, v.render(), v.n());
 				}
 			}
 		}
@@ -807,10 +862,10 @@ mixed_kernel(const MixedTable T, unsigned int *__restrict__ queue,
 		atomicAdd(steps, cnt);
 }
 
-template <int NF, typename V, bool ROLLED>
+template <int NF, typename V, bool ROLLED, bool UNI>
 cudaError_t
-launch_nf(const MixedTable &T, unsigned int *queue, unsigned long long *steps,
-          cudaStream_t st, const MixedLaunch &cfg)
+launch_nf(const MixedTable &T, const MixedRender &R1, unsigned int *queue,
+          unsigned long long *steps, cudaStream_t st, const MixedLaunch &cfg)
 {
 	const int maxb = Lanes<V>::N == 1 ? 256 : 128;
 	int block = cfg.block > 0 ? cfg.block : maxb;
@@ -819,7 +874,7 @@ launch_nf(const MixedTable &T, unsigned int *queue, unsigned long long *steps,
 	int per_sm = cfg.blocks_per_sm;
 	int occ = 0;
 	cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-		&occ, mixed_kernel<NF, V, ROLLED>, block, 0);
+		&occ, mixed_kernel<NF, V, ROLLED, UNI>, block, 0);
 	if(e != cudaSuccess)
 		return e;
 	if(per_sm <= 0 || per_sm > occ)
@@ -830,17 +885,24 @@ launch_nf(const MixedTable &T, unsigned int *queue, unsigned long long *steps,
 	unsigned grid = (unsigned)(want < need ? want : need);
 	if(grid == 0)
 		grid = 1;
-	mixed_kernel<NF, V, ROLLED><<<grid, block, 0, st>>>(T, queue, steps);
+	mixed_kernel<NF, V, ROLLED, UNI><<<grid, block, 0, st>>>(T, R1, queue, steps);
 	return cudaGetLastError();
 }
 
+/* The one-render form is built for the scalar, unrolled kernel alone: the
+ * other forms are autotuner alternatives. */
 template <typename V>
 cudaError_t
-launch_v(const MixedTable &T, int n_freq, unsigned int *queue, unsigned long long *steps,
-         cudaStream_t st, const MixedLaunch &cfg)
+launch_v(const MixedTable &T, const MixedRender *one, int n_freq, unsigned int *queue,
+         unsigned long long *steps, cudaStream_t st, const MixedLaunch &cfg)
 {
-#define LNF(NF) (cfg.rk4_rolled ? launch_nf<NF, V, true>(T, queue, steps, st, cfg) \
-                                : launch_nf<NF, V, false>(T, queue, steps, st, cfg))
+	MixedRender none;
+	memset(&none, 0, sizeof(none));
+	const bool uni = one && T.n_renders == 1 && Lanes<V>::N == 1 && !cfg.rk4_rolled;
+	const MixedRender &R1 = uni ? *one : none;
+#define LNF(NF) (cfg.rk4_rolled ? launch_nf<NF, V, true, false>(T, R1, queue, steps, st, cfg) \
+                 : uni ? launch_nf<NF, V, false, Lanes<V>::N == 1>(T, R1, queue, steps, st, cfg) \
+                       : launch_nf<NF, V, false, false>(T, R1, queue, steps, st, cfg))
 	switch(n_freq) {
 	case 0: return LNF(0);
 	case 1: return LNF(1);
@@ -861,23 +923,24 @@ cudaError_t
 occ_nf(int block, bool rolled, int *out)
 {
 	return rolled ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-	                    out, mixed_kernel<NF, V, true>, block, 0)
+	                    out, mixed_kernel<NF, V, true, false>, block, 0)
 	              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-	                    out, mixed_kernel<NF, V, false>, block, 0);
+	                    out, mixed_kernel<NF, V, false, false>, block, 0);
 }
 
 } /* namespace */
 
 cudaError_t
 launch_mixed_table(const MixedTable &T, int n_freq, unsigned int *queue,
-                   unsigned long long *steps, cudaStream_t st, const MixedLaunch &cfg)
+                   unsigned long long *steps, cudaStream_t st, const MixedLaunch &cfg,
+                   const MixedRender *one)
 {
 	cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned int), st);
 	if(e != cudaSuccess)
 		return e;
 	if(cfg.rays_per_thread == 2)
-		return launch_v<F2>(T, n_freq, queue, steps, st, cfg);
-	return launch_v<float>(T, n_freq, queue, steps, st, cfg);
+		return launch_v<F2>(T, one, n_freq, queue, steps, st, cfg);
+	return launch_v<float>(T, one, n_freq, queue, steps, st, cfg);
 }
 
 cudaError_t
@@ -957,9 +1020,19 @@ fill_mixed_render(const RenderParams &p, double *data, double *info, double t_in
 		m->nupow[i] = p.nupow_f[i];
 		m->nuinv2[i] = p.nuinv2_f[i];
 	}
+	m->n0t = p.flow == GRAY_FLOW_TORUS ? m->n0_rp15 : 0.0f;
+	m->kap0 = p.n_freq > 0 ? m->kappa * m->nuinv2[0] : 0.0f;
+	for(int i = 0; i < GRAY_MAX_FREQ; ++i) {
+		m->tcoef[i] = 0.0f;
+		if(i < p.n_freq) {
+			const double q = p.nu[0] / p.nu[i];
+			m->tcoef[i] = (float)(-1.4426950408889634 * (q * q));
+		}
+	}
 	m->flow = p.flow;
 	m->dump_begin = 0;
 	m->dump_end = (int)n_dump;
+	m->n_ticks = (int)((INT_MAX / n_sub) * n_sub);
 	m->a_d = p.a;
 	m->aa_d = p.aa;
 	m->rp_d = p.rp;

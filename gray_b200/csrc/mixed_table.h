@@ -34,9 +34,15 @@ struct MixedRender {
 	float  kappa, n0_rp15, ihr2_log2e;
 	float  nupow[GRAY_MAX_FREQ];
 	float  nuinv2[GRAY_MAX_FREQ];
+	/* the analytic torus folded for the Hamiltonian kernel: the density
+	 * scale (zero without the torus flow), kappa nu_0^-2, and
+	 * -log2(e) (nu_0/nu_i)^2, which turns tau_0 into -log2(e) tau_i */
+	float  n0t, kap0;
+	float  tcoef[GRAY_MAX_FREQ];
 	int    flow;
 	int    dump_begin;         /* integrate dump intervals [dump_begin,        */
 	int    dump_end;           /*   dump_end) of the render's schedule          */
+	int    n_ticks;            /* ticks per dump interval: a multiple of n_sub */
 	double a_d, aa_d, rp_d;    /* FP64 islands                                */
 	double *data, *info;       /* SoA FP64 state and getuu diagnostic         */
 	long long n_rays;
@@ -59,10 +65,14 @@ void fill_mixed_render(const RenderParams &p, double *data, double *info,
                        double t_init, double dt_dump, long long n_dump,
                        long long n_sub, MixedRender *m);
 
-/* rays_per_thread: 1 (scalar FP32) or 2 (two rays per thread in f32x2) */
+/* rays_per_thread: 1 (scalar FP32) or 2 (two rays per thread in f32x2).
+ * one (nullable): a host copy of the table's only render; with it, a
+ * one-render launch passes the render as a kernel parameter, so that its
+ * constants are read from the constant bank instead of held in registers
+ * per ray. */
 cudaError_t launch_mixed_table(const MixedTable &T, int n_freq, unsigned int *queue,
                                unsigned long long *steps, cudaStream_t st,
-                               const MixedLaunch &cfg);
+                               const MixedLaunch &cfg, const MixedRender *one = nullptr);
 
 /* numerical spacetime: every render of the table on the same grid and with
  * the same n_freq; inbox (nullable) accumulates the steps that interpolate
