@@ -33,6 +33,7 @@
  */
 #include <climits>
 #include <cstring>
+#include <type_traits>
 
 #include "gray_internal.h"
 #include "logk2_table.h"
@@ -164,25 +165,27 @@ template <> struct Lanes<F2> { static constexpr int N = 2; };
 /* ------------------------------------------------ per-ray render constants */
 
 /* Register layout of a ray in the mixed kernel: the event x^mu, the spatial
- * covariant momentum k_i, then I_nu and the optical depth of the first
- * frequency.  k_t is conserved (the metric does not depend on t) and lives
- * in RC.  For the torus every frequency's absorption is the same function
+ * covariant momentum k_i, then -I_nu and the optical depth of the first
+ * frequency.  The intensities are held negated (exactly, at load and store)
+ * because the transfer's dI_nu/dl is minus a power of 2: the registers then
+ * integrate that power of 2 itself.  k_t is conserved (the metric does not
+ * depend on t) and lives in RC.  For the torus every frequency's absorption is the same function
  * of the ray times nu_i^-2 (alpha_nu = kappa n nu^-2 at the fluid-frame
  * frequency, dtau_i = -alpha shift), so tau_i - tau_i(0) = (nu_0/nu_i)^2
  * (tau_0 - tau_0(0)) holds exactly and only tau_0 is integrated. */
 template <int NF>
 struct Layout {
 	static constexpr int NI = 7 + (NF > 0 ? NF + 1 : 0); /* integrated reals     */
-	static constexpr int I0 = 7;                        /* first I_nu           */
+	static constexpr int I0 = 7;                        /* first -I_nu          */
 	static constexpr int TAU = 7 + NF;                  /* tau of frequency 0   */
 	static constexpr int ND = 8 + 2 * NF;               /* reals in HBM per ray */
 };
 
 template <typename V, int NF>
 struct RC {
-	V a, aa, risco, n0t, ihr2, kap0, kt;
-	/* log2(nu_i^-0.7) plus the frequency's optical-depth offset, and the
-	 * factor turning tau_0 into -log2(e) tau_i */
+	V a, aa, risco, ihr2, ktau, kt;
+	/* log2(n0 r_+^1.5 nu_i^-0.7) plus the frequency's optical-depth
+	 * offset, and the factor turning tau_0 into -log2(e) tau_i */
 	V lgnu[NF > 0 ? NF : 1], tcoef[NF > 0 ? NF : 1];
 };
 
@@ -208,16 +211,15 @@ load_rc(RC<V, NF> &rc, int k, const MixedRender &c, double kt, const double *tau
 		setl(rc.a, k, c.a);
 		setl(rc.aa, k, c.aa);
 		setl(rc.risco, k, c.risco);
-		setl(rc.n0t, k, c.n0t);
 		setl(rc.ihr2, k, c.ihr2_log2e);
-		setl(rc.kap0, k, c.kap0);
+		setl(rc.ktau, k, c.ktau);
 	}
 	setl(rc.kt, k, (float)kt);
 #pragma unroll
 	for(int i = 0; i < NF; ++i) {
 		const double q = tau_ratio(c, i);
 		const double off = tau0[i] - q * tau0[0];
-		setl(rc.lgnu[i], k, log2f(c.nupow[i]) - (float)(1.4426950408889634 * off));
+		setl(rc.lgnu[i], k, (c.ln0t + log2f(c.nupow[i])) - (float)(1.4426950408889634 * off));
 		if constexpr(!UNI)
 			setl(rc.tcoef[i], k, c.tcoef[i]);
 	}
@@ -237,9 +239,8 @@ step_rc(const RC<V, NF> &rc, const MixedRender &R)
 		o.a = bc<V>(R.a);
 		o.aa = bc<V>(R.aa);
 		o.risco = bc<V>(R.risco);
-		o.n0t = bc<V>(R.n0t);
 		o.ihr2 = bc<V>(R.ihr2_log2e);
-		o.kap0 = bc<V>(R.kap0);
+		o.ktau = bc<V>(R.ktau);
 #pragma unroll
 		for(int i = 0; i < NF; ++i)
 			o.tcoef[i] = bc<V>(R.tcoef[i]);
@@ -322,10 +323,12 @@ ks_ham(const RC<V, NF> &c, const V *s, V *ds, Aux<V> &aux)
  * emission is masked to zero outside r_isco, where the Keplerian flow is
  * not timelike, or where the shift is not positive.  The shift is -k_mu
  * u^mu_fluid with k_mu straight from the state.  Every factor is folded into
- * one power of 2 per output:
- *   dtau_0 = -kappa nu_0^-2 n / shift
- *   dI_i   = -n nu_i^-0.7 shift^-2.7 e^-tau_i
- * with n = n0 (r_+/r)^1.5 exp(-z^2 / (2 (h r)^2)). */
+ * one power of 2 per output, with the density n = n0 r_+^1.5 2^ln in log2,
+ * ln = -1.5 lg2 r - z^2 log2(e) / (2 (h r)^2):
+ *   dtau_0  = -kappa nu_0^-2 n0 r_+^1.5 2^(ln - lg2 shift)
+ *   d(-I_i) = 2^(ln + lg2(n0 r_+^1.5 nu_i^-0.7) - 2.7 lg2 shift - log2(e) tau_i)
+ * (dI_i = -n nu_i^-0.7 shift^-2.7 e^-tau_i).  Where the emission is masked
+ * ln = -inf, which makes every output exactly 0. */
 template <typename V, int NF>
 __device__ __forceinline__ void
 torus_rt(const RC<V, NF> &c, const V *s, const Aux<V> &x, V *ds)
@@ -347,12 +350,12 @@ torus_rt(const RC<V, NF> &c, const V *s, const Aux<V> &x, V *ds)
 	ok = andv(ok, gtv(shift, zero));
 	V lsh = lg2v(selv(ok, shift, one));
 	V gz  = -((q3 * q3) * ((x.ir * x.ir) * c.ihr2));  /* log2 of the Gaussian */
-	V A   = selv(ok, -(c.n0t * (x.ir * irs)), zero);  /* -n0 (r_+/r)^1.5 */
-	ds[Y::TAU] = (A * c.kap0) * ex2v(gz - lsh);
-	V g27 = fmav(bc<V>(-2.7f), lsh, gz);
+	V ln  = selv(ok, fmav(bc<V>(-1.5f), lg2v(x.r), gz), bc<V>(-INFINITY));
+	ds[Y::TAU] = c.ktau * ex2v(ln - lsh);
+	V g27 = fmav(bc<V>(-2.7f), lsh, ln);
 #pragma unroll
 	for(int i = 0; i < NF; ++i)
-		ds[Y::I0 + i] = A * ex2v(fmav(s[Y::TAU], c.tcoef[i], g27 + c.lgnu[i]));
+		ds[Y::I0 + i] = ex2v(fmav(s[Y::TAU], c.tcoef[i], g27 + c.lgnu[i]));
 }
 
 template <typename V, int NF>
@@ -432,7 +435,7 @@ getuu_d(double a, const double *s)
 /* Scalar state of one ray slot (a thread has Lanes<V>::N slots). */
 struct Slot {
 	const MixedRender *c;
-	long long ray;
+	unsigned int ray;  /* a render has at most 2^31 rays */
 	int dump, dump_end, h, n, dh_cap;
 	float cdt;   /* n / |dt| */
 	float dtn;   /* dt / n   */
@@ -481,7 +484,7 @@ struct SlotView {
  * is kept out of line: its FP64 temporaries do not add to the register
  * count of the stepping loop. */
 __device__ __noinline__ void
-store_ray(const MixedRender &c, long long ray, int nf, const float *hi, const float *lo)
+store_ray(const MixedRender &c, unsigned int ray, int nf, const float *hi, const float *lo)
 {
 	const long long nr = c.n_rays;
 	double q[4], k[4], u[4];
@@ -509,7 +512,7 @@ store_ray(const MixedRender &c, long long ray, int nf, const float *hi, const fl
 		}
 		c.data[(8 + nf) * nr + ray] = tau;
 		for(int i = 0; i < nf; ++i)
-			c.data[(8 + i) * nr + ray] = (double)hi[7 + i] - (double)lo[7 + i];
+			c.data[(8 + i) * nr + ray] = (double)lo[7 + i] - (double)hi[7 + i]; /* I = -(hi - lo) */
 	}
 	double s[8] = {q[0], q[1], q[2], q[3], u[0], u[1], u[2], u[3]};
 	c.info[ray] = getuu_d(c.a_d, s);
@@ -527,6 +530,16 @@ store_slot(const MixedRender &c, const Slot &S, int k, const V *hi, const V *lo)
 		l[i] = getl(lo[i], k);
 	}
 	store_ray(c, S.ray, NF, h, l);
+}
+
+template <int L, typename C>
+__device__ __forceinline__ void
+flush_steps(C &cnt, unsigned long long *steps)
+{
+	if(L == 1 && cnt >= 0x80000000u) {
+		atomicAdd(steps, (unsigned long long)cnt);
+		cnt = 0;
+	}
 }
 
 /* Map a global queue index to (render, ray) by binary search over the
@@ -664,7 +677,10 @@ mixed_kernel(const MixedTable T, const __grid_constant__ MixedRender R1,
 	RC<V, NF> rc;
 	Slot S[L];
 	bool exhausted = false;
-	unsigned long long cnt = 0;
+	/* accepted steps of this thread; with one slot a 32-bit count, flushed
+	 * at a ray's events (store, dump boundary) once it reaches 2^31: between
+	 * two events a ray takes at most one interval's ticks (< 2^31) */
+	typename std::conditional<L == 1, unsigned int, unsigned long long>::type cnt = 0;
 #pragma unroll
 	for(int k = 0; k < L; ++k)
 		S[k].active = false;
@@ -698,7 +714,7 @@ mixed_kernel(const MixedTable T, const __grid_constant__ MixedRender R1,
 			const int rdx = UNI ? 0 : find_render(T, g);
 			const MixedRender &c = UNI ? R1 : T.renders[rdx];
 			Slot &s = S[k];
-			s.ray = (long long)(UNI ? g : g - T.prefix[rdx]);
+			s.ray = (unsigned int)(UNI ? g : g - T.prefix[rdx]);
 			s.dump = c.dump_begin;
 			if constexpr(!UNI) {
 				s.c = &c;
@@ -725,7 +741,7 @@ mixed_kernel(const MixedTable T, const __grid_constant__ MixedRender R1,
 			v[4] = k0[1]; v[5] = k0[2]; v[6] = k0[3];
 #pragma unroll
 			for(int i = 0; i < NF; ++i) {
-				v[Y::I0 + i] = c.data[(8 + i) * nr + s.ray];
+				v[Y::I0 + i] = -c.data[(8 + i) * nr + s.ray];
 				tau0[i] = c.data[(8 + NF + i) * nr + s.ray];
 			}
 			if(NF > 0)
@@ -760,6 +776,7 @@ mixed_kernel(const MixedTable T, const __grid_constant__ MixedRender R1,
 			if(dh[k] == 0) {
 				store_slot<V, NF>(v.render(), S[k], k, hi, lo);
 				S[k].active = false;
+				flush_steps<L>(cnt, steps);
 			} else {
 				step = true;
 			}
@@ -845,6 +862,7 @@ mixed_kernel(const MixedTable T, const __grid_constant__ MixedRender R1,
 			const SlotView<UNI> v{s, R1};
 			s.h += dh[k];
 			if(s.h >= v.n()) {
+				flush_steps<L>(cnt, steps);
 				if(++s.dump >= v.dump_end()) {
 					store_slot<V, NF>(v.render(), s, k, hi, lo);
 					s.active = false;
@@ -855,11 +873,12 @@ mixed_kernel(const MixedTable T, const __grid_constant__ MixedRender R1,
 		}
 	}
 
+	unsigned long long total = cnt;
 #pragma unroll
 	for(int o = 16; o > 0; o >>= 1)
-		cnt += __shfl_xor_sync(FULL, cnt, o);
-	if(lane == 0 && cnt)
-		atomicAdd(steps, cnt);
+		total += __shfl_xor_sync(FULL, total, o);
+	if(lane == 0 && total)
+		atomicAdd(steps, total);
 }
 
 template <int NF, typename V, bool ROLLED, bool UNI>
@@ -1020,8 +1039,11 @@ fill_mixed_render(const RenderParams &p, double *data, double *info, double t_in
 		m->nupow[i] = p.nupow_f[i];
 		m->nuinv2[i] = p.nuinv2_f[i];
 	}
-	m->n0t = p.flow == GRAY_FLOW_TORUS ? m->n0_rp15 : 0.0f;
-	m->kap0 = p.n_freq > 0 ? m->kappa * m->nuinv2[0] : 0.0f;
+	/* the density scale n0 r_+^1.5 (zero without the torus flow) in log2,
+	 * and -kappa nu_0^-2 n0 r_+^1.5 */
+	const float n0t = p.flow == GRAY_FLOW_TORUS ? m->n0_rp15 : 0.0f;
+	m->ln0t = n0t > 0.0f ? log2f(n0t) : -INFINITY;
+	m->ktau = p.n_freq > 0 ? -(m->kappa * m->nuinv2[0]) * n0t : 0.0f;
 	for(int i = 0; i < GRAY_MAX_FREQ; ++i) {
 		m->tcoef[i] = 0.0f;
 		if(i < p.n_freq) {

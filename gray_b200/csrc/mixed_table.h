@@ -34,10 +34,11 @@ struct MixedRender {
 	float  kappa, n0_rp15, ihr2_log2e;
 	float  nupow[GRAY_MAX_FREQ];
 	float  nuinv2[GRAY_MAX_FREQ];
-	/* the analytic torus folded for the Hamiltonian kernel: the density
-	 * scale (zero without the torus flow), kappa nu_0^-2, and
-	 * -log2(e) (nu_0/nu_i)^2, which turns tau_0 into -log2(e) tau_i */
-	float  n0t, kap0;
+	/* the analytic torus folded for the Hamiltonian kernel: log2 of the
+	 * density scale n0 r_+^1.5 (-inf without the torus flow),
+	 * -kappa nu_0^-2 n0 r_+^1.5, and -log2(e) (nu_0/nu_i)^2, which turns
+	 * tau_0 into -log2(e) tau_i */
+	float  ln0t, ktau;
 	float  tcoef[GRAY_MAX_FREQ];
 	int    flow;
 	int    dump_begin;         /* integrate dump intervals [dump_begin,        */
