@@ -15,13 +15,16 @@ Metric: ray-steps/s = accepted RK4 steps summed over rays / time.
               plus the device-to-host copy of the final state every step
   roofline    FP32 CUDA-core bound (the path has no dense contraction);
               peak = FMA-loop microbenchmark measured in this run
-  cpu_baseline  the C oracle on the host cores, bounded ray sample
+  cpu_baseline  the C oracle on the host cores, bounded ray sample, with the
+              reference's own compiled program timed on the same rays
 
 --impl reference times the reference's CPU implementation of the path:
 the reference's OpenCL build cannot run here (no OpenCL platform, no lux
 runtime, and its analytic Kerr-Schild kernel does not compile as shipped),
-so its restatement in oracle/ (test/baseline infrastructure) is timed with
-every host thread on a bounded sample of the same workload.
+so its own .cl program, compiled for the host from its sources under an
+OpenCL shim (oracle/_ref), is timed with every host thread on a bounded
+sample of the same rays; its FP64 restatement in oracle/ (which also runs
+the workload's torus transfer) is timed beside it.
 
 Multi-GPU (torchrun): every rank renders its own copy of the workload
 (independent renders, weak scaling); the only collective is the max-over-
@@ -53,7 +56,7 @@ METRIC = "ray-steps/s"
 
 # DRAM bytes (read + write) of one full-size launch of the dominant kernel,
 # from one-pass ncu captures (dram__bytes_read.sum + dram__bytes_write.sum).
-TRAFFIC = {"torus_rt_1024": 151332352 + 143093504,
+TRAFFIC = {"torus_rt_1024": 149105664 + 127566848,
            "numerical_128": 500394240 + 17862656}
 # Host-to-device bytes of one render through the C ABI: the render's table
 # entry (sizeof(MixedRender) in gray_b200/csrc/mixed_table.h), which the
@@ -172,29 +175,73 @@ def analytic_cpu(cfg, args, fp32=True):
         res["fp32"] = dict({"value": int(s32.sum()) / t32, "unit": "ray-steps/s",
                             "note": "every real in float (the reference's default "
                                     "precision); does not meet the 1e-4 image bar"}, **extra)
+    if O.ref_available():
+        value, secs, nparts = reference_program_cpu(cfg, rays, K, threads)
+        res["reference_program"] = {"value": value, "unit": "ray-steps/s", "cores": threads,
+                                    "kind": "reference", "program": REF_PROGRAM_NOTE,
+                                    "seconds": secs}
     return res
 
 
+REF_PROGRAM_NOTE = ("the reference's analytic Kerr-Schild program (sim-org KS.cl, rt.cl, "
+                    "phys.cl, RK4.cl, driver.cl) compiled from its own sources for the host "
+                    "(oracle/_ref); its analytic spacetime has no flow (flow.cl reads a "
+                    "numerical grid's rho), so it integrates the same geodesics and step "
+                    "control with one frequency of rt.cl transfer at zero emission")
+
+
+def reference_program_cpu(cfg, rays, K, threads):
+    """The reference's own analytic program over the fixed sample on every
+    host thread, timed in K interleaved parts; its driver loop's accepted
+    steps are counted by the build (they equal the oracle's)."""
+    O = oracle()
+    parts = cpu_time(lambda r, t: O.ref_ks_trace(cfg, r, nthreads=t, with_steps=True)[2],
+                     rays, K, threads)
+    steps, secs = sum(p[0] for p in parts), sum(p[1] for p in parts)
+    return steps / secs, secs, len(parts)
+
+
 def reference_arm(args, cfg, rank):
-    """The reference's CPU implementation of the path (the FP64 restatement
-    in oracle/, see the module docstring) on every host thread.  Each bench
-    step is one interleaved part of the fixed ray sample, so the K timed
-    steps together cover the whole sample: the same rays and arithmetic as
-    the cpu_baseline leg of the GPU arm, timed the same way."""
+    """The reference's CPU implementation of the path on every host thread:
+    its own analytic program (oracle/_ref) where it was compiled, else the
+    FP64 restatement in oracle/.  Each bench step is one interleaved part of
+    the fixed ray sample, so the K timed steps together cover the whole
+    sample.  The restatement, which also runs the workload's torus transfer,
+    is timed beside it on the same rays."""
     if rank != 0:
+        return
+    if args.workload in ("numerical_128",):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "numerical_128's grid is generated on the GPU; its CPU baseline is "
+                          "the cpu_baseline leg of the GPU arm's line"}), flush=True)
         return
     O = oracle()
     threads = os.cpu_count() or 1
     n_rays = cfg["n_width"] * cfg["n_height"]
     rays = cpu_sample(n_rays, args.cpu_rays)
     K = max(args.steps, 1)
-    trace = lambda r, t: O.trace(cfg, r, nthreads=t)[2]  # noqa: E731
     warm = rays[::max(K, 1)][:max(threads, 1)]
+    port = lambda r, t: O.trace(cfg, r, nthreads=t)[2]  # noqa: E731
     for _ in range(args.warmup):
-        trace(warm, threads)
-    parts = cpu_time(trace, rays, K, threads)
-    steps, secs = sum(p[0] for p in parts), sum(p[1] for p in parts)
-    value = steps / secs
+        port(warm, threads)
+    parts = cpu_time(port, rays, K, threads)
+    psteps, psecs = sum(p[0] for p in parts), sum(p[1] for p in parts)
+    port_line = {"value": psteps / psecs, "unit": "ray-steps/s", "cores": threads,
+                 "kind": "port", "precision": "fp64",
+                 "note": "the oracle's restatement with the workload's transfer"}
+    sample = "%d rays of %s (prime stride %d), every dump interval" % (
+        rays.size, args.workload, CPU_STRIDE)
+    if O.ref_available():
+        for _ in range(args.warmup):
+            O.ref_ks_trace(cfg, warm, nthreads=threads)
+        value, secs, nparts = reference_program_cpu(cfg, rays, K, threads)
+        base = {"value": value, "unit": "ray-steps/s", "cores": threads, "kind": "reference",
+                "precision": "fp64", "program": REF_PROGRAM_NOTE,
+                "sample": sample + ", %.1f s in %d parts" % (secs, nparts), "port": port_line}
+    else:
+        value, secs = port_line["value"], psecs
+        base = dict(port_line, sample=sample + ", %.1f s in %d parts" % (psecs, len(parts)))
+        base.pop("note")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "ray-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -202,11 +249,7 @@ def reference_arm(args, cfg, rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "rays_per_render": n_rays,
                    "sample": "fixed strided rays", "precision": "fp64"},
-        "cpu_baseline": {"value": value, "unit": "ray-steps/s", "cores": threads,
-                         "kind": "port",
-                         "sample": "%d rays of %s (prime stride %d), every dump interval, "
-                                   "%.1f s in %d parts" % (rays.size, args.workload, CPU_STRIDE,
-                                                          secs, len(parts))},
+        "cpu_baseline": base,
         "e2e": {"value": value, "unit": "ray-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }

@@ -496,9 +496,10 @@ def ref_ks_func(name, a, q, u=None):
     return f(ctypes.c_double(a), _p(q))
 
 
-def ref_ks_trace(cfg, rays):
+def ref_ks_trace(cfg, rays, nthreads=1, with_steps=False):
     """icond_drv + evolve_drv of the reference's analytic program over the
-    listed rays: (states [n, 8], info [n])."""
+    listed rays on nthreads host threads (0: all): (states [n, 8], info [n])
+    and, with_steps, the accepted RK4 steps of each ray."""
     L = _reflib("libref_ks.so")
     d = RefKsDesc(cfg.get("a_spin", 0.0), cfg.get("w_img", 64.0), cfg.get("h_img", 64.0),
                   cfg.get("r_obs", 1024.0), cfg.get("i_obs", 60.0), cfg.get("j_obs", 0.0),
@@ -506,10 +507,13 @@ def ref_ks_trace(cfg, rays):
                   cfg.get("dt_dump", -32.0), cfg.get("n_sub", 1024), cfg.get("n_dump", 64))
     rays = np.ascontiguousarray(rays, dtype=np.int64)
     out, info = np.zeros((rays.size, 8)), np.zeros(rays.size)
+    steps = np.zeros(rays.size, dtype=np.int64)
+    if nthreads <= 0:
+        nthreads = os.cpu_count() or 1
     if L.ref_ks_trace(ctypes.byref(d), _pi(rays), ctypes.c_int64(rays.size), _p(out),
-                      _p(info)) != 0:
+                      _p(info), _pi(steps), ctypes.c_int(nthreads)) != 0:
         raise ValueError("ray index outside the image")
-    return out, info
+    return (out, info, steps) if with_steps else (out, info)
 
 
 def ref_dyst_trace(cfg, levels, box, rays):

@@ -15,8 +15,8 @@
  *    spacetime does not have: the overload here returns a flow with no
  *    electrons (n_e = 0), so the transfer state stays zero.
  * The entry points run icond_drv and evolve_drv over a list of rays, one
- * work-item at a time, as the reference's host loop (sim-org/gray.c:243-294)
- * drives them dump by dump.
+ * work-item at a time per host thread, as the reference's host loop
+ * (sim-org/gray.c:243-294) drives them dump by dump.
  */
 #include "opencl_shim.h"
 
@@ -63,7 +63,20 @@ template <typename... A> struct flow getflow(real4, real4, A...)
 #include "rt.cl"
 #include "AoS.cl"
 #include "phys.cl"
+
+/* RK4.cl's integrate() under another name, and a forwarding integrate()
+ * that counts the calls: driver.cl calls it once per accepted step, so the
+ * count is the ray-steps of the reference's own loop */
+thread_local long long ref_steps;
+#define integrate ref_integrate
 #include "RK4.cl"
+#undef integrate
+template <typename... A> struct state integrate(struct state s, real dt, A... a)
+{
+	++ref_steps;
+	return ref_integrate(s, dt, a...);
+}
+
 #include "driver.cl"
 
 } /* namespace ref_ks */
@@ -110,9 +123,11 @@ void ref_ks_rhs(double a, const double *s, double *ds)
 }
 
 /* icond_drv + evolve_drv per dump for the listed rays: out [n][8] (x^mu,
- * u^mu), info [n], the state after n_dump intervals */
+ * u^mu), info [n], the state after n_dump intervals; steps [n] (nullable)
+ * the accepted RK4 steps of each ray.  nthreads host threads share the
+ * list (at least one). */
 int ref_ks_trace(const ref_ks_desc *d, const int64_t *rays, int64_t n, double *out,
-                 double *info)
+                 double *info, int64_t *steps, int nthreads)
 {
 	a_spin = d->a_spin;
 	w_rays_v = (size_t)d->w_rays;
@@ -145,13 +160,19 @@ int ref_ks_trace(const ref_ks_desc *d, const int64_t *rays, int64_t n, double *o
 	          g_tt_t2 = {}, g_tx_t2 = {}, g_ty_t2 = {}, g_tz_t2 = {}, g_xx_t2 = {},
 	          g_xy_t2 = {}, g_xz_t2 = {}, g_yy_t2 = {}, g_yz_t2 = {}, g_zz_t2 = {},
 	          rho_t2 = {};
+	for(int64_t j = 0; j < n; ++j)
+		if(rays[j] < 0 || (size_t)rays[j] >= n_rays)
+			return -1;
+	/* the whole render's arrays, as the reference allocates them; each
+	 * work-item touches only its own ray's slots, so the listed rays can
+	 * run on several threads at once */
 	std::vector<real> data((size_t)n_data * n_rays), inf((size_t)n_info * n_rays);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads > 0 ? nthreads : 1)
 	for(int64_t j = 0; j < n; ++j) {
 		const int64_t g = rays[j];
-		if(g < 0 || (size_t)g >= n_rays)
-			return -1;
 		gray_shim_gid[0] = (size_t)(g / d->w_rays); /* gj: row    */
 		gray_shim_gid[1] = (size_t)(g % d->w_rays); /* gi: column */
+		const long long s0 = ref_steps;
 		icond_drv(data.data(), inf.data(), d->w_img, d->h_img, d->r_obs, d->i_obs, d->j_obs,
 		          nullptr, SPACETIME_ARGS);
 		/* sim-org/gray.c:248-257: one evolve per dump interval */
@@ -164,6 +185,8 @@ int ref_ks_trace(const ref_ks_desc *d, const int64_t *rays, int64_t n, double *o
 		for(int s = 0; s < 8; ++s)
 			out[j * 8 + s] = data[(size_t)g * n_data + s];
 		info[j] = inf[(size_t)g];
+		if(steps)
+			steps[j] = (int64_t)(ref_steps - s0);
 	}
 	return 0;
 }

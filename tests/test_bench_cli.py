@@ -1,6 +1,7 @@
-"""bench.py's reference arm (the oracle port on the host cores) runs without
-a GPU: check its JSON line on a short run, and that ranks other than 0 of a
-multi-rank launch exit quietly."""
+"""bench.py's reference arm (the reference's own program compiled for the
+host, with the oracle port beside it) runs without a GPU: check its JSON
+line on a short run, and that ranks other than 0 of a multi-rank launch
+exit quietly."""
 import json
 import os
 import subprocess
@@ -22,7 +23,15 @@ def test_reference_arm_line():
     line = json.loads(p.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["metric"] == "ray-steps/s"
     assert line["value"] > 0 and line["higher_is_better"] is True
-    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    base = line["cpu_baseline"]
+    assert base["cores"] >= 1
+    if O.ref_available():  # the reference's own program, the restatement beside it
+        assert base["kind"] == "reference" and base["port"]["kind"] == "port"
+        assert base["port"]["value"] > 0
+    else:
+        assert base["kind"] == "port"
     assert line["e2e"] == {"value": line["value"], "unit": "ray-steps/s",
                            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert line["config"]["workload"] == "torus_rt_1024"
@@ -38,8 +47,10 @@ def test_reference_arm_other_ranks_exit_quietly():
 def test_cpu_legs_time_one_fixed_sample():
     """The GPU arm's cpu_baseline leg and the reference arm time the same
     fixed ray sample (the same indices, every dump interval) split the same
-    way, so their rates differ only by timing noise; the FP32 build of the
-    restatement is reported beside the FP64 one with its image error."""
+    way, with the same programs (the restatement, and the reference's own
+    program where it was built), so their rates differ only by timing noise;
+    the FP32 build of the restatement is reported beside the FP64 one with
+    its image error."""
     import argparse
     import sys
     sys.path.insert(0, ROOT)
@@ -54,6 +65,11 @@ def test_cpu_legs_time_one_fixed_sample():
     assert res["kind"] == "port" and res["precision"] == "fp64" and res["value"] > 0
     assert "64 rays" in res["sample"] and "in 3 parts" in res["sample"]
     assert res["fp32"]["value"] > 0 and res["fp32"]["image_rel_l2_err_vs_fp64"] > 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if O.ref_available():
+        assert res["reference_program"]["kind"] == "reference"
+        assert res["reference_program"]["value"] > 0
     p = run(["--impl", "reference", "--steps", "3", "--warmup", "3", "--cpu-rays", "64",
              "--side", "32"])
     assert p.returncode == 0, p.stderr[-2000:]

@@ -69,6 +69,25 @@ def test_ks_traces_are_the_references():
     assert np.max(np.abs(ginfo - rinfo) / norm) <= 1e-14
 
 
+def test_reference_loop_steps_and_threads():
+    """The reference's driver loop counts the same accepted RK4 steps per ray
+    as the oracle (kerr_small_64, and the first rays of the torus_rt_1024
+    CPU sample), and its multi-threaded run equals the single-threaded one."""
+    cfg = configs.KERR_SMALL_64
+    rays = (np.arange(64, dtype=np.int64) * 61) % (64 * 64)
+    one, info1 = O.ref_ks_trace(cfg, rays)
+    many, info_m, steps = O.ref_ks_trace(cfg, rays, nthreads=4, with_steps=True)
+    assert np.array_equal(one, many) and np.array_equal(info1, info_m)
+    _, _, osteps = O.trace(cfg, rays)
+    assert np.array_equal(steps, osteps)
+    cfg = configs.TORUS_RT_1024
+    rays = (np.arange(24, dtype=np.int64) * 7919) % (1024 * 1024)
+    ref, _, steps = O.ref_ks_trace(cfg, rays, nthreads=0, with_steps=True)
+    got, _, osteps = O.trace(cfg, rays)
+    assert np.array_equal(steps, osteps)
+    assert np.max(np.abs(got[:, :8] - ref) / np.abs(ref).max(axis=1, keepdims=True)) <= 1e-8
+
+
 def test_ks_trace_a_zero_spin_and_forward():
     """a = 0 and a forward (dt > 0) trace, two dumps."""
     cfg = dict(configs.scaled(configs.KERR_SMALL_64, 6), a_spin=0.0, r_obs=60.0, i_obs=80.0,
