@@ -225,6 +225,18 @@ typedef int sampler_t;
 #define CLK_ADDRESS_CLAMP_TO_EDGE 2
 #define CLK_FILTER_LINEAR 16
 
+#ifdef GRAY_SHIM_NO_IMAGES
+/* A program that reads no image (the analytic spacetime): the image type is
+ * empty, so the 102 image arguments every kernel function passes on
+ * (preamble.cl's SPACETIME_PROTOTYPE_ARGS) cost nothing to copy, as in an
+ * OpenCL build where they are handles. */
+struct image3d_t {
+};
+inline real4 read_imagef(image3d_t, sampler_t, real4)
+{
+	return real4{0, 0, 0, 1};
+}
+#else
 /* a 3-D single-channel FP32 image: one field of a grid level, read from
  * an interleaved [z][y][x][stride] array at offset comp */
 struct image3d_t {
@@ -260,6 +272,7 @@ inline real4 read_imagef(image3d_t im, sampler_t, real4 c)
 	         ax * w[1] * w[2] * T(i0[0], i1[1], i1[2]) + w[0] * w[1] * w[2] * T(i1[0], i1[1], i1[2]);
 	return r;
 }
+#endif /* GRAY_SHIM_NO_IMAGES */
 
 /* --------------------------------------------------------------- work items */
 

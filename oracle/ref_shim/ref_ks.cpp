@@ -18,6 +18,7 @@
  * work-item at a time per host thread, as the reference's host loop
  * (sim-org/gray.c:243-294) drives them dump by dump.
  */
+#define GRAY_SHIM_NO_IMAGES /* the analytic program reads no image */
 #include "opencl_shim.h"
 
 #include <cstdlib>
