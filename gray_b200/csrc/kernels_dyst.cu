@@ -574,65 +574,50 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 	float dtn = 0.0f;
 	double dtnd = 0.0; /* the FP64 substep unit of the transfer */
 	bool active = false, exhausted = false;
-	/* all steps; steps that interpolate.  32-bit, flushed at a ray's dump
-	 * boundaries once they reach 2^31: between two boundaries a ray takes at
-	 * most one interval's ticks (< 2^31) */
-	unsigned int cnt = 0, cnt_in = 0;
+	unsigned long long cnt = 0, cnt_in = 0; /* all steps; steps that interpolate */
 	const MixedRender *c = nullptr;
 
 	for(;;) {
-		/* refill (one vote per step while every lane of the warp is busy) */
-		if(!__all_sync(FULL, active)) {
-			bool need = !active && !exhausted;
-			unsigned mask = __ballot_sync(FULL, need);
-			if(mask) {
-				int leader = __ffs(mask) - 1;
-				unsigned base = 0;
-				if(lane == leader)
-					base = atomicAdd(queue, (unsigned)__popc(mask));
-				base = __shfl_sync(FULL, base, leader);
-				if(need) {
-					unsigned long long gidx = (unsigned long long)base +
-					                          __popc(mask & ((1u << lane) - 1));
-					if(gidx < T.total) {
-						int rr = 0;
-						while(rr + 1 < T.n_renders && T.prefix[rr + 1] <= gidx)
-							++rr;
-						c = &T.renders[rr];
-						ray = (long long)(gidx - T.prefix[rr]);
-						n = (int)((INT_MAX / c->n_sub) * c->n_sub);
+		bool need = !active && !exhausted;
+		unsigned mask = __ballot_sync(FULL, need);
+		if(mask) {
+			int leader = __ffs(mask) - 1;
+			unsigned base = 0;
+			if(lane == leader)
+				base = atomicAdd(queue, (unsigned)__popc(mask));
+			base = __shfl_sync(FULL, base, leader);
+			if(need) {
+				unsigned long long gidx = (unsigned long long)base +
+				                          __popc(mask & ((1u << lane) - 1));
+				if(gidx < T.total) {
+					int rr = 0;
+					while(rr + 1 < T.n_renders && T.prefix[rr + 1] <= gidx)
+						++rr;
+					c = &T.renders[rr];
+					ray = (long long)(gidx - T.prefix[rr]);
+					n = (int)((INT_MAX / c->n_sub) * c->n_sub);
 #pragma unroll
-						for(int k = 0; k < ND; ++k) {
-							double v = c->data[k * c->n_rays + ray];
-							hi[k] = (float)v;
-							lo[k] = (float)((double)hi[k] - v);
-						}
-#pragma unroll
-						for(int k = 0; k < NR; ++k)
-							rt[k] = c->data[(ND + k) * c->n_rays + ray];
-						dump = c->dump_begin - 1;
-						h = n; /* forces the first dump set-up below */
-						active = true;
-					} else {
-						exhausted = true;
+					for(int k = 0; k < ND; ++k) {
+						double v = c->data[k * c->n_rays + ray];
+						hi[k] = (float)v;
+						lo[k] = (float)((double)hi[k] - v);
 					}
+#pragma unroll
+					for(int k = 0; k < NR; ++k)
+						rt[k] = c->data[(ND + k) * c->n_rays + ray];
+					dump = c->dump_begin - 1;
+					h = n; /* forces the first dump set-up below */
+					active = true;
+				} else {
+					exhausted = true;
 				}
 			}
-			if(!__any_sync(FULL, active))
-				break;
 		}
+		if(!__any_sync(FULL, active))
+			break;
 		if(!active)
 			continue;
 		if(h >= n) { /* next dump interval: constants of driver.cl:93 */
-			if(cnt >= 0x80000000u) {
-				atomicAdd(steps, (unsigned long long)cnt);
-				cnt = 0;
-			}
-			if(cnt_in >= 0x80000000u) {
-				if(inbox)
-					atomicAdd(inbox, (unsigned long long)cnt_in);
-				cnt_in = 0;
-			}
 			if(++dump >= c->dump_end) {
 				double s[ND];
 #pragma unroll
@@ -750,16 +735,15 @@ dyst_mixed_kernel(const MixedTable T, const GridParams g, const DystConst dc,
 			active = false;
 		}
 	}
-	unsigned long long all = cnt, in = cnt_in;
 #pragma unroll
 	for(int o = 16; o > 0; o >>= 1) {
-		all += __shfl_xor_sync(FULL, all, o);
-		in += __shfl_xor_sync(FULL, in, o);
+		cnt += __shfl_xor_sync(FULL, cnt, o);
+		cnt_in += __shfl_xor_sync(FULL, cnt_in, o);
 	}
-	if(lane == 0 && all)
-		atomicAdd(steps, all);
-	if(lane == 0 && in && inbox)
-		atomicAdd(inbox, in);
+	if(lane == 0 && cnt)
+		atomicAdd(steps, cnt);
+	if(lane == 0 && cnt_in && inbox)
+		atomicAdd(inbox, cnt_in);
 }
 
 template <int NF, bool STAGED>
