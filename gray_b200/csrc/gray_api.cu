@@ -1183,9 +1183,12 @@ gray_batch_destroy(gray_ctx *c, int id)
 }
 
 /* Enqueue the batch: initial conditions of every render, counters reset,
- * one persistent launch over the whole table. */
+ * one persistent launch over the whole table.  one: the host copy of the
+ * table's entry when the batch holds one render (the one-render launch),
+ * else null. */
 static int
-batch_enqueue(gray_ctx *c, Batch *b, const MixedLaunch &cfg, const MixedTable &T)
+batch_enqueue(gray_ctx *c, Batch *b, const MixedLaunch &cfg, const MixedTable &T,
+              const MixedRender *one)
 {
 	for(int id : b->ids) {
 		Render *r = find(c, id);
@@ -1199,7 +1202,7 @@ batch_enqueue(gray_ctx *c, Batch *b, const MixedLaunch &cfg, const MixedTable &T
 		CK(launch_dyst_mixed_table(T, c->grid->gp, b->n_freq, b->d_queue, b->d_steps,
 		                           c->stream, cfg));
 	else
-		CK(launch_mixed_table(T, b->n_freq, b->d_queue, b->d_steps, c->stream, cfg));
+		CK(launch_mixed_table(T, b->n_freq, b->d_queue, b->d_steps, c->stream, cfg, one));
 	return GRAY_OK;
 }
 
@@ -1241,7 +1244,8 @@ gray_batch_run(gray_ctx *c, int id, double *ns)
 		/* capture once; the graph is replayed by every later run */
 		cudaGraph_t g = nullptr;
 		CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-		int st = batch_enqueue(c, b, c->mixed, batch_table(b));
+		int st = batch_enqueue(c, b, c->mixed, batch_table(b),
+		                       b->host_table.size() == 1 ? &b->host_table[0] : nullptr);
 		cudaError_t e = cudaStreamEndCapture(c->stream, &g);
 		if(st) {
 			if(g)
@@ -1380,7 +1384,7 @@ gray_plan(gray_ctx *c, int id, int flags, gray_launch_plan *best)
 			double ns = 0.0;
 			if((st = timed_begin(c)))
 				break;
-			if((st = batch_enqueue(c, b, cand[k], T)))
+			if((st = batch_enqueue(c, b, cand[k], T, trial.size() == 1 ? &trial[0] : nullptr)))
 				break;
 			if((st = timed_end(c, &ns)))
 				break;

@@ -135,7 +135,8 @@ gray_run_mixed_noalloc(int device, const gray_render_desc *descs, int n_renders,
 		T.total = total;
 		/* the context's default plan: one ray per thread, 256 threads */
 		MixedLaunch cfg = {256, 0, sms, 1};
-		e = launch_mixed_table(T, n_freq, &S->queue, &S->steps, st, cfg);
+		e = launch_mixed_table(T, n_freq, &S->queue, &S->steps, st, cfg,
+		                       n_renders == 1 ? &table[0] : nullptr);
 	}
 	if(e == cudaSuccess && steps_host) {
 		unsigned long long v = 0;

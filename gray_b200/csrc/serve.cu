@@ -206,7 +206,8 @@ iterate(Server *S, std::vector<Request *> &fresh)
 			e = launch_dyst_mixed_table(T, c->grid->gp, g - NUM_GROUP, q, S->d_steps + g,
 			                            S->s[1], dc);
 		} else {
-			e = launch_mixed_table(T, g, q, S->d_steps + g, S->s[0], cfg);
+			e = launch_mixed_table(T, g, q, S->d_steps + g, S->s[0], cfg,
+			                       count[g] == 1 ? &S->h_tab[start[g]] : nullptr);
 		}
 		if(e != cudaSuccess)
 			return gi_from_cuda(e);
