@@ -401,9 +401,9 @@ int gray_run_series(gray_ctx *ctx, int render, const gray_grid_desc *grid,
  *  - The kernel's scratch (render table, ray queue, step counter:
  *    GRAY_NOALLOC_SCRATCH_BYTES) is a static device array that every GPU
  *    loading this library holds until exit.  The first call on a device
- *    looks up its address (cudaGetSymbolAddress); make that first call
- *    before any stream capture.  Every call shares the array: calls that
- *    overlap on the GPU (other streams, other host threads) race.
+ *    looks up its address (cudaGetSymbolAddress).  Every call shares the
+ *    array: calls that overlap on the GPU (other streams, other host
+ *    threads) race.
  *  - Work is enqueued on cuda_stream (a cudaStream_t, NULL = legacy default
  *    stream).  If steps_host is non-NULL the call waits and stores the
  *    accepted ray-steps there; otherwise it returns after enqueueing. */
