@@ -47,6 +47,28 @@ def test_batch_equals_renders_alone(ctx):
             r.close()
 
 
+def test_one_render_batch_and_table_constants_agree(ctx):
+    """A batch of one render runs the one-render launch (the render's
+    constants as a kernel parameter) inside its graph; a batch of two reads
+    each ray's constants from the table into registers.  Both equal the
+    renders run alone bit for bit."""
+    cfgs = small_survey(n=2)
+    ref = [alone(ctx, c) for c in cfgs]
+    for group in ([cfgs[0]], cfgs):
+        rs = [ctx.render(dict(c, precision=api.PREC_MIXED)) for c in group]
+        b = ctx.batch(rs)
+        try:
+            for rep in range(2):
+                b.run()
+                assert b.steps() == sum(s for _, s in ref[:len(group)])
+                for r, (d, _) in zip(rs, ref):
+                    assert np.array_equal(r.state(api.LAYOUT_AOS)[0], d), (len(group), rep)
+        finally:
+            b.close()
+            for r in rs:
+                r.close()
+
+
 def test_rays_per_thread_variants_agree(ctx):
     """Packed two-ray and scalar kernels, RK4 stages unrolled or looped: the
     looped stages run the same operations in the same order."""

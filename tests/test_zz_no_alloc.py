@@ -75,6 +75,32 @@ def test_noalloc_matches_ordinary_entry_point(ctx):
             assert np.max(np.abs(gi - info)) <= TOL * max(1.0, np.max(np.abs(info)))
 
 
+def test_noalloc_one_render(ctx):
+    """One render: the call's launch takes the render's constants as a
+    kernel parameter; the result is the ordinary entry point's."""
+    import torch
+
+    cfg = dict(configs.scaled(configs.TORUS_RT_1024, 32), a_spin=0.9, i_obs=45.0)
+    data, info, steps_ref = reference_run(ctx, cfg)
+    desc = (api.RenderDesc * 1)(api.make_desc(dict(cfg, precision=api.PREC_MIXED)))
+    nr = cfg["n_width"] * cfg["n_height"]
+    state = torch.full((8 + 2 * len(cfg["nu"]), nr), float("nan"), dtype=torch.float64,
+                       device="cuda")
+    inf = torch.full((nr,), float("nan"), dtype=torch.float64, device="cuda")
+    sp = (ctypes.c_void_p * 1)(state.data_ptr())
+    ip = (ctypes.c_void_p * 1)(inf.data_ptr())
+    steps = ctypes.c_uint64(0)
+    torch.cuda.synchronize()
+    st = api.lib().gray_run_mixed_noalloc(torch.cuda.current_device(), desc, 1, sp, ip,
+                                          ctypes.c_void_p(0), ctypes.byref(steps))
+    assert st == api.OK, api.strerror(st)
+    torch.cuda.synchronize()
+    assert steps.value == steps_ref
+    scale = np.maximum(np.abs(data), 1e-300).max(axis=1, keepdims=True)
+    assert np.max(np.abs(state.cpu().numpy() - data) / scale) <= TOL
+    assert np.max(np.abs(inf.cpu().numpy() - info)) <= TOL * max(1.0, np.max(np.abs(info)))
+
+
 def test_noalloc_rejects_sizes_beyond_the_scratch():
     L = api.lib()
     n = api.NOALLOC_MAX_RENDERS + 1
