@@ -96,7 +96,7 @@ def parse():
                          "scaling); survey_256 split: the renders are divided across ranks; "
                          "torus_rt_1024 rows: each rank integrates a contiguous row block "
                          "of the one render and rank 0 gathers the state (strong scaling)")
-    ap.add_argument("--dumps-per-iter", type=int, default=16,
+    ap.add_argument("--dumps-per-iter", type=int, default=4,
                     help="serve_mix: dump intervals each server iteration advances")
     return ap.parse_args()
 

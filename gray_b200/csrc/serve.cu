@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -64,6 +65,28 @@ struct Request {
 		return p.spacetime == GRAY_ST_NUMERICAL ? NUM_GROUP + p.n_freq : p.n_freq;
 	}
 };
+
+/* Estimated seconds of one dump interval of a render on the shared device:
+ * its steps per interval times the longer of one ray's step latency (a
+ * small render's rays each run alone in a warp) and its rays' share of the
+ * device's throughput.  The figures are B200 measurements of the mixed
+ * kernels (analytic, numerical); they only size windows and never change a
+ * result. */
+constexpr double STEP_LATENCY_S[2] = {1.5e-6, 9e-6};
+constexpr double STEP_COST_S[2] = {1.0 / 4.5e10, 1.0 / 1.4e10};
+constexpr double MIN_ITER_S = 0.05;
+
+double
+interval_s(const Request *r)
+{
+	const int k = r->p.spacetime == GRAY_ST_NUMERICAL ? 1 : 0;
+	const double n_sub = (double)r->desc.n_sub;
+	/* steps per interval: the analytic cap |dt|/n_sub (phys.cl:60-61; more
+	 * near the horizon); the numerical spacetime's step is
+	 * min(|dt|/n_sub, 0.01) (dyst.cl:43-53 gives eps = 1) */
+	const double steps = k ? std::max(n_sub, std::fabs(r->desc.dt_dump) / 0.01) : n_sub;
+	return steps * std::max(STEP_LATENCY_S[k], (double)r->p.n_rays * STEP_COST_S[k]);
+}
 
 } /* namespace */
 
@@ -143,19 +166,20 @@ iterate(Server *S, std::vector<Request *> &fresh)
 		return GRAY_OK;
 
 	/* 2. one table per group, entries with the next window of dumps.  The
-	 * largest admitted render advances dumps_per_iter intervals; a smaller
-	 * one advances as many intervals as the same ray-intervals of work
-	 * allow (at most the ones it has left), so it finishes in fewer
-	 * iterations while the iteration's length stays set by the largest */
+	 * iteration lasts dumps_per_iter intervals of the admitted render with
+	 * the longest estimated interval (and at least MIN_ITER_S); every render
+	 * advances as many intervals as fit in that time (at most the ones it
+	 * has left), so small renders finish in an iteration or two while a
+	 * newcomer waits at most about one iteration for admission */
 	const int dpi = S->cfg.dumps_per_iter;
-	long long max_rays = 1;
+	double t_iter = MIN_ITER_S;
 	for(Request *r : S->inflight)
-		max_rays = std::max(max_rays, r->p.n_rays);
+		t_iter = std::max(t_iter, dpi * interval_s(r));
 	for(Request *r : S->inflight) {
-		const double w = (double)dpi * (double)max_rays / (double)std::max(1LL, r->p.n_rays);
+		const double w = t_iter / interval_s(r);
 		const int left = (int)r->desc.n_dump - r->next_dump;
 		/* left = 0 (no dump intervals): an empty window, the render is done */
-		r->window = left <= 0 ? 0 : std::min(left, w < (double)left ? std::max(dpi, (int)w) : left);
+		r->window = left <= 0 ? 0 : (w < (double)left ? std::max(dpi, (int)w) : left);
 	}
 	int count[GROUPS] = {0}, start[GROUPS];
 	for(Request *r : S->inflight)

@@ -252,10 +252,14 @@ int gray_get_plan(const gray_ctx *ctx, gray_launch_plan *plan);
  * (the configured budget) and table slots free up, and advances every
  * admitted render by a window of dump intervals per iteration: one
  * persistent launch per kind (analytic by n_freq, numerical), so renders
- * that arrived while others run share the device with them.  The largest
- * admitted render advances dumps_per_iter intervals; a render with fewer
- * rays advances as many more as keep its work (rays x intervals) at the
- * largest one's, so small renders finish within an iteration or two.  Finished
+ * that arrived while others run share the device with them.  An iteration
+ * lasts dumps_per_iter intervals of the admitted render whose interval is
+ * estimated to take longest (and at least 50 ms); every other render
+ * advances as many intervals as fit in that time, so small renders finish
+ * within an iteration or two and a newcomer waits about one iteration at
+ * most for admission.  The estimates (steps per interval times the longer
+ * of one ray's step latency and the rays' share of the device) size the
+ * windows only; results do not depend on them.  Finished
  * renders are copied to host memory and their device state is freed.  Only
  * mixed-precision renders are served; numerical ones use the context's
  * grid, which must be loaded before gray_serve_start.  While the server
