@@ -85,6 +85,9 @@ struct gray_ctx {
 int  gi_from_cuda(cudaError_t e);
 int  gi_dalloc(gray_ctx *c, void **p, size_t bytes);
 void gi_dfree(gray_ctx *c, void *p, size_t bytes);
+/* the HBM budget without an allocation (memory from the server's pool) */
+int  gi_reserve(gray_ctx *c, size_t bytes);
+void gi_unreserve(gray_ctx *c, size_t bytes);
 int  gi_grid_ready(gray_ctx *c);
 Render *gi_find_render(gray_ctx *c, int id);
 int  gi_icond(gray_ctx *c, Render *r);

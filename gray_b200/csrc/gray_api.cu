@@ -216,6 +216,23 @@ gi_dalloc(gray_ctx *c, void **p, size_t bytes)
 	return dalloc(c, p, bytes);
 }
 
+int
+gi_reserve(gray_ctx *c, size_t bytes)
+{
+	std::lock_guard<std::mutex> lk(c->mem_mu);
+	if(c->used + bytes > c->budget)
+		return GRAY_EBUDGET;
+	c->used += bytes;
+	return GRAY_OK;
+}
+
+void
+gi_unreserve(gray_ctx *c, size_t bytes)
+{
+	std::lock_guard<std::mutex> lk(c->mem_mu);
+	c->used -= bytes;
+}
+
 void
 gi_dfree(gray_ctx *c, void *p, size_t bytes)
 {

@@ -23,10 +23,12 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <iterator>
 #include <map>
 #include <mutex>
 #include <new>
 #include <thread>
+#include <utility>
 #include <vector>
 
 #include "ctx_internal.h"
@@ -46,6 +48,31 @@ now_s()
 	return duration<double>(steady_clock::now() - t0).count();
 }
 
+/* An allocator whose value-construction leaves the elements uninitialised:
+ * a finished render's host buffers are overwritten by the device copy at
+ * once, so zero-filling them first (over 100 MB for a 1024^2 render) would
+ * only hold up the scheduler. */
+template <typename T>
+struct NoInit : std::allocator<T> {
+	template <typename U>
+	struct rebind {
+		typedef NoInit<U> other;
+	};
+	NoInit() = default;
+	template <typename U>
+	NoInit(const NoInit<U> &) noexcept {}
+	template <typename U, typename... A>
+	void construct(U *p, A &&...a)
+	{
+		::new((void *)p) U(std::forward<A>(a)...);
+	}
+	template <typename U>
+	void construct(U *p) noexcept
+	{
+		::new((void *)p) U;
+	}
+};
+
 struct Request {
 	uint64_t id = 0;
 	gray_render_desc desc;
@@ -58,11 +85,22 @@ struct Request {
 	int next_dump = 0;
 	int window = 0;  /* dump intervals of the current iteration */
 	std::atomic<bool> cancel{false}; /* set by gray_serve_cancel, read by the scheduler */
-	std::vector<double> h_data, h_info;
+	/* a finished render's state and info: a block of the server's pinned
+	 * pool (hres, at hres_off) or, when the pool has no room, vectors */
+	char *hres = nullptr;
+	size_t hres_off = 0;
+	std::vector<double, NoInit<double>> h_data, h_info;
 
 	int group() const
 	{
 		return p.spacetime == GRAY_ST_NUMERICAL ? NUM_GROUP + p.n_freq : p.n_freq;
+	}
+	size_t data_count() const { return (size_t)p.n_rays * p.n_data; }
+	size_t result_bytes() const { return (data_count() + (size_t)p.n_rays) * sizeof(double); }
+	const double *res_data() const { return hres ? (const double *)hres : h_data.data(); }
+	const double *res_info() const
+	{
+		return hres ? (const double *)hres + data_count() : h_info.data();
 	}
 };
 
@@ -76,16 +114,24 @@ constexpr double STEP_LATENCY_S[2] = {1.5e-6, 9e-6};
 constexpr double STEP_COST_S[2] = {1.0 / 4.5e10, 1.0 / 1.4e10};
 constexpr double MIN_ITER_S = 0.05;
 
+/* steps of one ray per interval: the analytic cap |dt|/n_sub
+ * (phys.cl:60-61; more near the horizon); the numerical spacetime's step
+ * is min(|dt|/n_sub, 0.01) (dyst.cl:43-53 gives eps = 1) */
+double
+interval_steps(const Request *r)
+{
+	const double n_sub = (double)r->desc.n_sub;
+	return r->p.spacetime == GRAY_ST_NUMERICAL
+	           ? std::max(n_sub, std::fabs(r->desc.dt_dump) / 0.01)
+	           : n_sub;
+}
+
 double
 interval_s(const Request *r)
 {
 	const int k = r->p.spacetime == GRAY_ST_NUMERICAL ? 1 : 0;
-	const double n_sub = (double)r->desc.n_sub;
-	/* steps per interval: the analytic cap |dt|/n_sub (phys.cl:60-61; more
-	 * near the horizon); the numerical spacetime's step is
-	 * min(|dt|/n_sub, 0.01) (dyst.cl:43-53 gives eps = 1) */
-	const double steps = k ? std::max(n_sub, std::fabs(r->desc.dt_dump) / 0.01) : n_sub;
-	return steps * std::max(STEP_LATENCY_S[k], (double)r->p.n_rays * STEP_COST_S[k]);
+	return interval_steps(r) *
+	       std::max(STEP_LATENCY_S[k], (double)r->p.n_rays * STEP_COST_S[k]);
 }
 
 } /* namespace */
@@ -106,6 +152,18 @@ struct Server {
 	gray_serve_stats stats;
 	/* device: table | prefix | 2 counters per group */
 	void *dblock = nullptr;
+	/* the requests' device state: stream-ordered allocations from a pool
+	 * that keeps its memory, so admitting and retiring a render neither
+	 * maps nor unmaps HBM nor synchronises the device (cudaMalloc and
+	 * cudaFree of large states stalled the scheduler for up to a second) */
+	cudaMemPool_t pool = nullptr;
+	/* pinned host pool for finished renders' results: the scheduler's copy
+	 * out of HBM then runs at full speed into memory that is already
+	 * mapped, instead of faulting in fresh pageable pages (which stalled
+	 * every other request for up to a second per large render) */
+	char *hpool = nullptr;
+	size_t hpool_bytes = 0;
+	std::map<size_t, size_t> hfree; /* offset -> bytes of each free block */
 	size_t dbytes = 0;
 	MixedRender *d_tab = nullptr;
 	unsigned long long *d_pre = nullptr;
@@ -121,11 +179,67 @@ struct Server {
 
 namespace {
 
+constexpr size_t HPOOL_BYTES = size_t(2) << 30;
+
+size_t
+pool_round(size_t bytes)
+{
+	return (bytes + 255) & ~size_t(255);
+}
+
+/* First fit in the pinned pool (S->mu held); nullptr when nothing fits. */
+char *
+pool_take(Server *S, size_t bytes, size_t *off)
+{
+	bytes = pool_round(bytes);
+	for(auto it = S->hfree.begin(); it != S->hfree.end(); ++it) {
+		if(it->second < bytes)
+			continue;
+		const size_t at = it->first, rest = it->second - bytes;
+		S->hfree.erase(it);
+		if(rest) {
+			try {
+				S->hfree[at + bytes] = rest;
+			} catch(const std::bad_alloc &) {
+				/* the remainder is lost to the pool until the server stops */
+			}
+		}
+		*off = at;
+		return S->hpool + at;
+	}
+	return nullptr;
+}
+
+/* Return a block to the pool, merged with free neighbours (S->mu held). */
+void
+pool_give(Server *S, size_t off, size_t bytes)
+{
+	bytes = pool_round(bytes);
+	auto next = S->hfree.lower_bound(off);
+	if(next != S->hfree.end() && off + bytes == next->first) {
+		bytes += next->second;
+		next = S->hfree.erase(next);
+	}
+	if(next != S->hfree.begin()) {
+		auto prev = std::prev(next);
+		if(prev->first + prev->second == off) {
+			prev->second += bytes;
+			return;
+		}
+	}
+	try {
+		S->hfree[off] = bytes;
+	} catch(const std::bad_alloc &) {
+		/* lost to the pool until the server stops */
+	}
+}
+
 void
 release(Server *S, Request *r)
 {
 	if(r->d_data) {
-		gi_dfree(S->c, r->d_data, r->bytes);
+		cudaFreeAsync(r->d_data, S->s[0]); /* after the stream's copies of it */
+		gi_unreserve(S->c, r->bytes);
 		r->d_data = r->d_info = nullptr;
 		S->inflight_bytes -= r->bytes;
 	}
@@ -139,7 +253,16 @@ iterate(Server *S, std::vector<Request *> &fresh)
 	cudaError_t e = cudaSuccess;
 	/* 1. admission: state + initial conditions of the fresh requests */
 	for(Request *r : fresh) {
-		int st = gi_dalloc(c, (void **)&r->d_data, r->bytes);
+		/* on the stream of its kind's launches, which use it first; the
+		 * retiring copies on s[0] wait for s[1] */
+		cudaStream_t st_ = S->s[r->group() >= NUM_GROUP ? 1 : 0];
+		int st = gi_reserve(c, r->bytes);
+		if(!st && cudaMallocFromPoolAsync((void **)&r->d_data, r->bytes, S->pool, st_) !=
+		              cudaSuccess) {
+			cudaGetLastError();
+			gi_unreserve(c, r->bytes);
+			st = GRAY_ENOMEM;
+		}
 		if(st) {
 			std::lock_guard<std::mutex> lk(S->mu);
 			r->state = GRAY_REQ_FAILED;
@@ -155,7 +278,6 @@ iterate(Server *S, std::vector<Request *> &fresh)
 		/* in flight before its first launch, so that a failure below frees
 		 * it with the rest (the capacity was reserved at start) */
 		S->inflight.push_back(r);
-		cudaStream_t st_ = S->s[r->group() >= NUM_GROUP ? 1 : 0];
 		e = r->group() >= NUM_GROUP
 		        ? launch_dyst_icond(r->p, c->grid->gp, r->d_data, r->d_info, st_)
 		        : launch_icond64(r->p, r->d_data, r->d_info, st_);
@@ -191,7 +313,15 @@ iterate(Server *S, std::vector<Request *> &fresh)
 	int fill[GROUPS];
 	unsigned long long total[GROUPS] = {0};
 	memcpy(fill, start, sizeof(fill));
-	for(Request *r : S->inflight) {
+	/* within a group, the renders whose rays take longest this iteration
+	 * (window x steps per interval) first in the queue: a small render's
+	 * few long rays then start with the iteration instead of after a large
+	 * render's many short ones (longest processing time first) */
+	std::vector<Request *> order(S->inflight);
+	std::stable_sort(order.begin(), order.end(), [](const Request *a, const Request *b) {
+		return a->window * interval_steps(a) > b->window * interval_steps(b);
+	});
+	for(Request *r : order) {
 		int g = r->group(), k = fill[g]++;
 		MixedRender &m = S->h_tab[k];
 		memset(&m, 0, sizeof(m));
@@ -257,13 +387,26 @@ iterate(Server *S, std::vector<Request *> &fresh)
 	}
 	for(Request *r : done) {
 		if(!r->cancel) {
-			const size_t nr = (size_t)r->p.n_rays;
-			r->h_data.resize(nr * r->p.n_data);
-			r->h_info.resize(nr);
-			if((e = cudaMemcpyAsync(r->h_data.data(), r->d_data, r->h_data.size() * sizeof(double),
-			                        cudaMemcpyDeviceToHost, S->s[0])) != cudaSuccess ||
-			   (e = cudaMemcpyAsync(r->h_info.data(), r->d_info, nr * sizeof(double),
-			                        cudaMemcpyDeviceToHost, S->s[0])) != cudaSuccess ||
+			const size_t nr = (size_t)r->p.n_rays, nd = r->data_count();
+			{
+				std::lock_guard<std::mutex> lk(S->mu);
+				if(S->hpool)
+					r->hres = pool_take(S, r->result_bytes(), &r->hres_off);
+			}
+			double *hd, *hi;
+			if(r->hres) {
+				hd = (double *)r->hres;
+				hi = hd + nd;
+			} else {
+				r->h_data.resize(nd);
+				r->h_info.resize(nr);
+				hd = r->h_data.data();
+				hi = r->h_info.data();
+			}
+			if((e = cudaMemcpyAsync(hd, r->d_data, nd * sizeof(double), cudaMemcpyDeviceToHost,
+			                        S->s[0])) != cudaSuccess ||
+			   (e = cudaMemcpyAsync(hi, r->d_info, nr * sizeof(double), cudaMemcpyDeviceToHost,
+			                        S->s[0])) != cudaSuccess ||
 			   (e = cudaStreamSynchronize(S->s[0])) != cudaSuccess)
 				return gi_from_cuda(e);
 		}
@@ -378,12 +521,19 @@ free_server(Server *S)
 	gray_ctx *c = S->c;
 	for(Request *r : S->inflight)
 		release(S, r);
+	for(int i = 0; i < 2; ++i)
+		if(S->s[i])
+			cudaStreamSynchronize(S->s[i]);
+	if(S->pool)
+		cudaMemPoolDestroy(S->pool);
 	for(auto &kv : S->reqs)
 		delete kv.second;
 	if(S->dblock)
 		gi_dfree(c, S->dblock, S->dbytes);
 	if(S->h_tab)
 		cudaFreeHost(S->h_tab);
+	if(S->hpool) /* after the requests whose results it held */
+		cudaFreeHost(S->hpool);
 	for(int i = 0; i < 2; ++i)
 		if(S->s[i])
 			cudaStreamDestroy(S->s[i]);
@@ -460,6 +610,33 @@ gray_serve_start(gray_ctx *c, const gray_serve_config *cfg)
 			S->h_tab = (MixedRender *)h;
 			S->h_pre = (unsigned long long *)((char *)h + tab);
 			S->h_steps = (unsigned long long *)((char *)h + tab + pre);
+		}
+		if(e == cudaSuccess) {
+			/* the result pool; without it results go to pageable memory */
+			S->hpool_bytes = std::min(HPOOL_BYTES, pool_round(S->budget));
+			if(cudaHostAlloc((void **)&S->hpool, S->hpool_bytes, cudaHostAllocDefault) ==
+			   cudaSuccess) {
+				try {
+					S->hfree[0] = S->hpool_bytes;
+				} catch(const std::bad_alloc &) {
+					cudaFreeHost(S->hpool);
+					S->hpool = nullptr;
+				}
+			} else {
+				cudaGetLastError();
+				S->hpool = nullptr;
+			}
+		}
+		if(e == cudaSuccess) {
+			cudaMemPoolProps pp;
+			memset(&pp, 0, sizeof(pp));
+			pp.allocType = cudaMemAllocationTypePinned;
+			pp.location.type = cudaMemLocationTypeDevice;
+			pp.location.id = c->device;
+			e = cudaMemPoolCreate(&S->pool, &pp);
+			uint64_t keep = UINT64_MAX; /* the budget bounds what it holds */
+			if(e == cudaSuccess)
+				e = cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep);
 		}
 		for(int i = 0; i < 2 && e == cudaSuccess; ++i)
 			e = cudaStreamCreateWithFlags(&S->s[i], cudaStreamNonBlocking);
@@ -568,27 +745,38 @@ gray_serve_result(gray_ctx *c, uint64_t id, void *data, size_t data_bytes, void 
 	if(!c->server)
 		return GRAY_ESTATE;
 	Server *S = c->server;
-	std::lock_guard<std::mutex> lk(S->mu);
-	auto it = S->reqs.find(id);
-	if(it == S->reqs.end())
-		return GRAY_ENOTFOUND;
-	Request *r = it->second;
-	if(r->state == GRAY_REQ_QUEUED || r->state == GRAY_REQ_RUNNING)
-		return GRAY_ESTATE;
+	Request *r = nullptr;
+	{
+		std::lock_guard<std::mutex> lk(S->mu);
+		auto it = S->reqs.find(id);
+		if(it == S->reqs.end())
+			return GRAY_ENOTFOUND;
+		r = it->second;
+		if(r->state == GRAY_REQ_QUEUED || r->state == GRAY_REQ_RUNNING)
+			return GRAY_ESTATE;
+		if(r->state == GRAY_REQ_DONE) {
+			if(data && data_bytes != r->data_count() * sizeof(double))
+				return GRAY_ESIZE;
+			if(info && info_bytes != (size_t)r->p.n_rays * sizeof(double))
+				return GRAY_ESIZE;
+		}
+		S->reqs.erase(it); /* the request is this caller's from here on */
+	}
+	/* the copies run without the server mutex: the scheduler never waits
+	 * for a client's memcpy */
 	if(r->state == GRAY_REQ_DONE) {
-		if(data && data_bytes != r->h_data.size() * sizeof(double))
-			return GRAY_ESIZE;
-		if(info && info_bytes != r->h_info.size() * sizeof(double))
-			return GRAY_ESIZE;
 		if(data)
-			memcpy(data, r->h_data.data(), data_bytes);
+			memcpy(data, r->res_data(), data_bytes);
 		if(info)
-			memcpy(info, r->h_info.data(), info_bytes);
+			memcpy(info, r->res_info(), info_bytes);
 	}
 	int st = r->state == GRAY_REQ_DONE ? GRAY_OK
 	         : r->state == GRAY_REQ_FAILED ? (r->status ? r->status : GRAY_ECUDA)
 	                                        : GRAY_ESTATE;
-	S->reqs.erase(it);
+	if(r->hres) {
+		std::lock_guard<std::mutex> lk(S->mu);
+		pool_give(S, r->hres_off, r->result_bytes());
+	}
 	delete r;
 	return st;
 }
