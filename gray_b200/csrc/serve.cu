@@ -245,6 +245,35 @@ release(Server *S, Request *r)
 	}
 }
 
+/* The SMs of the two kinds' persistent launches, which run at the same
+ * time on their two streams.  Each launch sizes its grid to its SM count,
+ * so with both kinds in flight neither grid takes the whole device and the
+ * other kind's launch does not wait for it to drain.  While the numerical
+ * renders' rays fit on at most half the SMs at once (2 blocks of 256 per
+ * SM), they get the SMs that hold them all: their windows were sized for
+ * rays that run at once.  Otherwise the SMs are split by the kinds'
+ * estimated work this iteration. */
+void
+split_sms(const Server *S, const unsigned long long *total, int *ana_sms, int *num_sms)
+{
+	const int sms = S->c->sms;
+	double work[2] = {0.0, 0.0};
+	for(const Request *r : S->inflight)
+		work[r->p.spacetime == GRAY_ST_NUMERICAL ? 1 : 0] += r->window * interval_s(r);
+	unsigned long long blocks = 0;
+	for(int g = NUM_GROUP; g < GROUPS; ++g)
+		blocks += (total[g] + 255) / 256;
+	*ana_sms = *num_sms = sms;
+	if(work[0] <= 0.0 || work[1] <= 0.0 || sms < 2)
+		return;
+	int n = (int)std::min<unsigned long long>((blocks + 1) / 2, (unsigned long long)sms);
+	if(n > sms / 2)
+		n = (int)std::lround(sms * work[1] / (work[0] + work[1]));
+	n = std::max(1, std::min(sms - 1, n));
+	*num_sms = n;
+	*ana_sms = sms - n;
+}
+
 /* Device-side work of one iteration.  Returns a GRAY_* status. */
 int
 iterate(Server *S, std::vector<Request *> &fresh)
@@ -345,6 +374,8 @@ iterate(Server *S, std::vector<Request *> &fresh)
 		return gi_from_cuda(e);
 	MixedLaunch cfg = c->mixed;
 	cfg.sms = c->sms;
+	int num_sms = c->sms;
+	split_sms(S, total, &cfg.sms, &num_sms);
 	for(int g = 0; g < GROUPS; ++g) {
 		if(!count[g])
 			continue;
@@ -357,6 +388,7 @@ iterate(Server *S, std::vector<Request *> &fresh)
 		if(g >= NUM_GROUP) {
 			MixedLaunch dc = cfg;
 			dc.block = 256;
+			dc.sms = num_sms;
 			e = launch_dyst_mixed_table(T, c->grid->gp, g - NUM_GROUP, q, S->d_steps + g,
 			                            S->s[1], dc);
 		} else {
