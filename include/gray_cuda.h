@@ -259,8 +259,12 @@ int gray_get_plan(const gray_ctx *ctx, gray_launch_plan *plan);
  * within an iteration or two and a newcomer waits about one iteration at
  * most for admission.  The estimates (steps per interval times the longer
  * of one ray's step latency and the rays' share of the device) size the
- * windows only; results do not depend on them.  Finished
- * renders are copied to host memory and their device state is freed.  Only
+ * windows only; results do not depend on them.  With analytic and
+ * numerical renders in flight at once, their two launches run together on
+ * a split of the SMs.  Request state comes from a device memory pool that
+ * the server keeps until it stops (its size never exceeds the budget).
+ * Finished renders are copied to host memory (a 2 GiB pinned pool while it
+ * has room) and their device state returns to the pool.  Only
  * mixed-precision renders are served; numerical ones use the context's
  * grid, which must be loaded before gray_serve_start.  While the server
  * runs, only gray_serve_* may be called on the context (they are
