@@ -438,6 +438,7 @@ struct Slot {
 	unsigned int ray;  /* a render has at most 2^31 rays */
 	int dump, dump_end, h, n, dh_cap;
 	float cdt;   /* n / |dt| */
+	float r2_far; /* x^2+y^2+z^2-a^2 beyond which the step is surely dh_cap */
 	float dtn;   /* dt / n   */
 	float rp, eps_stop, cdt_scale;
 	double aa_d, rp_d;
@@ -458,6 +459,12 @@ start_dump(Slot &S, const MixedRender &c, int n)
 	S.cdt    = (float)((double)n / fabs(dt));
 	S.dtn    = (float)(dt / (double)n);
 	S.h      = 0;
+	/* eps at which the tick rule reaches dh_cap, with 1% to spare for the
+	 * FP32 rounding of the exact rule: r^2 >= x^2+y^2+z^2-a^2 (KS.cl:48-55),
+	 * so beyond this the step is dh_cap whatever eps rounds to */
+	const double e_cap = sqrt((double)S.dh_cap / (0.01 * (double)S.cdt));
+	const double r_far = 1.01 * ((double)c.rp_d + e_cap) + 1.0;
+	S.r2_far = (float)(r_far * r_far);
 }
 
 /* A slot's render-wide values: from the slot (loaded with the ray) or, with
@@ -568,7 +575,10 @@ ticks(const SlotView<UNI> &v, int k, const V *hi, const V *lo)
 	float x = getl(hi[1], k), y = getl(hi[2], k), z = getl(hi[3], k);
 	float aa = (float)v.aa_d();
 	float zz = z * z;
-	float kk = 0.5f * (fmaf(x, x, fmaf(y, y, zz)) - aa);
+	float q2 = fmaf(x, x, fmaf(y, y, zz));
+	if(q2 - aa >= S.r2_far) /* far from the hole: the capped step */
+		return S.dh_cap < v.n() - S.h ? S.dh_cap : v.n() - S.h;
+	float kk = 0.5f * (q2 - aa);
 	float rr = sqrt_a(fmaf(kk, kk, aa * zz)) + kk;
 	float eps = sqrt_a(rr) - v.rp();
 	if(eps < 1.0f) {

@@ -21,7 +21,10 @@ integrated in Hamiltonian form on (x^mu, k_i) with k_t conserved:
                         (nu_0/nu_i)^2 times it
   RK4 + Kahan     per integrated real: stages 2 + 4 + 4, final 2 + 4
                   (Kahan) = 16, plus 3 scalars; 7 + (n_freq + 1) reals
-  step control    17  (FP32 radius root and the n/|dt| tick rule)
+  step control    6   (far from the hole, nearly every step of these
+                        workloads: x^2+y^2+z^2-a^2 against the per-interval
+                        bound beyond which the step is the cap; near it the
+                        FP32 radius root and the n/|dt| tick rule add 17)
 
 FP64 kernel (gray_b200/csrc/kernels_fp64.cu), per call:
   ks_rhs64        196  (5 divides and 2 sqrt counted as 1 each)
@@ -37,7 +40,7 @@ The reference's own comments count the same KS RHS as about 205 FLOP
 def mixed_per_step(n_freq, transfer=True):
     ni = 7 + (n_freq + 1 if n_freq else 0)
     rhs = 93 + ((35 + 4 * n_freq) if (transfer and n_freq) else 0)
-    return 4 * rhs + 16 * ni + 3 + 17
+    return 4 * rhs + 16 * ni + 3 + 6
 
 
 def fp64_per_step(n_freq, transfer=True):
