@@ -188,3 +188,24 @@ def test_windows_sized_by_time_and_empty_requests(ctx):
         assert stats.iterations <= 5
     finally:
         ctx.serve_stop()
+
+
+def test_results_beyond_the_pinned_pool(ctx):
+    """Finished results wait in the server's pinned host pool while it has
+    room (the pool is the budget's size below 2 GiB) and in pageable memory
+    beyond it; read results give their blocks back.  Every result, from
+    either place, equals the render run alone."""
+    cfgs = [dict(configs.scaled(configs.TORUS_RT_1024, s), n_dump=8) for s in (40, 24, 32, 16)]
+    sizes = [c["n_width"] * c["n_height"] * (8 + 2 * len(c["nu"]) + 1) * 8 for c in cfgs]
+    ref = [alone(ctx, c) for c in cfgs]
+    ctx.serve_start(hbm_budget=max(sizes) + min(sizes), dumps_per_iter=8)
+    try:
+        for rep in range(2):  # the second round reuses the blocks the first gave back
+            ids = [ctx.submit(c) for c in cfgs]
+            assert all(s == api.REQ_DONE for s in wait(ctx, ids))  # none read yet
+            for rid, c, (d, info) in zip(ids, cfgs, ref):
+                got, ginfo = ctx.result(rid, 8 + 2 * len(c["nu"]), c["n_width"] * c["n_height"])
+                scale = np.maximum(np.abs(d), 1e-300).max(axis=1, keepdims=True)
+                assert np.max(np.abs(got - d) / scale) <= 1e-6, rep
+    finally:
+        ctx.serve_stop()
