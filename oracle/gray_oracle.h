@@ -65,7 +65,7 @@ typedef struct {
 	int    nx, ny, nz;
 	float  box[8];             /* {t1, xmin, ymin, zmin, t2, xmax, ymax, zmax} */
 	const float *fields[2];    /* time levels t1, t2 */
-	int    bug_gzz;            /* 1: reproduce dyst.cl:283 (g_zz read as g_yz) */
+	int    bug_gzz;            /* 1: reproduce dyst.cl:78 (g_zz read as g_yz) */
 	int    physics;            /* 1: flat outside the box, time factor in [0,1] */
 } orc_grid;
 
