@@ -252,7 +252,7 @@ step_rc(const RC<V, NF> &rc, const MixedRender &R)
 
 template <typename V>
 struct Aux {
-	V r, ir, f, iss, R2;
+	V r, ir, f, iss, R2, lz; /* lz = z / r */
 };
 
 /* The geodesic equation of KS.cl:263-378 in Hamiltonian form.  With
@@ -316,7 +316,7 @@ ks_ham(const RC<V, NF> &c, const V *s, V *ds, Aux<V> &aux)
 	ds[5] = fmav(Gxy, y, fLi * fmav(r, ky, a * kx));
 	ds[6] = fmav(Gz, z, fmav(fL * ir, kz, hLL * fz));
 
-	aux.r = r; aux.ir = ir; aux.f = f; aux.iss = iss; aux.R2 = R2;
+	aux.r = r; aux.ir = ir; aux.f = f; aux.iss = iss; aux.R2 = R2; aux.lz = lz;
 }
 
 /* Torus flow + transfer (the FP64 kernel's model), branch-free: the
@@ -336,7 +336,7 @@ torus_rt(const RC<V, NF> &c, const V *s, const Aux<V> &x, V *ds)
 	typedef Layout<NF> Y;
 	typedef typename MaskOf<V>::T M;
 	const V one = bc<V>(1.0f), zero = bc<V>(0.0f);
-	const V q1 = s[1], q2 = s[2], q3 = s[3];
+	const V q1 = s[1], q2 = s[2];
 	const V kx = s[4], ky = s[5];
 	V irs = rsqv(x.r);                 /* r^-1/2 */
 	V sr  = x.r * irs;                 /* r^1/2  */
@@ -349,7 +349,7 @@ torus_rt(const RC<V, NF> &c, const V *s, const Aux<V> &x, V *ds)
 	V shift = -(utf * fmav(Om, fmav(q1, ky, -(q2 * kx)), c.kt));
 	ok = andv(ok, gtv(shift, zero));
 	V lsh = lg2v(selv(ok, shift, one));
-	V gz  = -((q3 * q3) * ((x.ir * x.ir) * c.ihr2));  /* log2 of the Gaussian */
+	V gz  = -((x.lz * x.lz) * c.ihr2);  /* log2 of the Gaussian: -(z/r)^2 log2(e) / (2 h^2) */
 	V ln  = selv(ok, fmav(bc<V>(-1.5f), lg2v(x.r), gz), bc<V>(-INFINITY));
 	ds[Y::TAU] = c.ktau * ex2v(ln - lsh);
 	V g27 = fmav(bc<V>(-2.7f), lsh, ln);

@@ -12,9 +12,10 @@ integrated in Hamiltonian form on (x^mu, k_i) with k_t conserved:
                         df/dz with 2 rsqrt + 2 rcp; l, L = l^mu k_mu,
                         dL/dr and the force G d_i r + f L (explicit d_i L),
                         and dx^mu/dl 61)
-  torus_rt        35 + 4 per frequency  (Keplerian flow and shift from
+  torus_rt        33 + 4 per frequency  (Keplerian flow and shift from
                         k_mu 23; the density in log2, -1.5 lg2 r plus the
-                        Gaussian, and dtau_0 as one ex2 12; per frequency
+                        Gaussian from z/r of the geodesic part, and dtau_0 as
+                        one ex2 10; per frequency
                         one ex2 of the summed log2 factors, with n0 and
                         nu_i^-0.7 folded into a per-ray constant 4); only
                         tau_0 is integrated, the other optical depths are
@@ -39,7 +40,7 @@ The reference's own comments count the same KS RHS as about 205 FLOP
 
 def mixed_per_step(n_freq, transfer=True):
     ni = 7 + (n_freq + 1 if n_freq else 0)
-    rhs = 93 + ((35 + 4 * n_freq) if (transfer and n_freq) else 0)
+    rhs = 93 + ((33 + 4 * n_freq) if (transfer and n_freq) else 0)
     return 4 * rhs + 16 * ni + 3 + 6
 
 
