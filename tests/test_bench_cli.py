@@ -37,6 +37,15 @@ def test_reference_arm_line():
     assert line["config"]["workload"] == "torus_rt_1024"
 
 
+def test_reference_arm_numerical_is_unavailable():
+    """numerical_128's grid is generated on the GPU, so the reference arm
+    says so on one line and exits 0 instead of timing the wrong program."""
+    p = run(["--impl", "reference", "--workload", "numerical_128", "--steps", "1", "--warmup", "3"])
+    assert p.returncode == 0, p.stderr[-2000:]
+    line = json.loads(p.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and "unavailable" in line
+
+
 def test_reference_arm_other_ranks_exit_quietly():
     p = run(["--impl", "reference", "--steps", "1", "--warmup", "3", "--gpus", "2"],
             env={"RANK": "1", "LOCAL_RANK": "1", "WORLD_SIZE": "2"})
