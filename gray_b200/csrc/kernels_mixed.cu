@@ -27,7 +27,8 @@
  *    rule (phys.cl:48-64) read it, and the null-constraint diagnostic
  *    (KS.cl:164-168) is computed in FP64 from the final state;
  *  - the integer-tick substep loop of driver.cl:81-99 is kept, so dump
- *    boundaries are hit exactly as in the FP64 kernel;
+ *    boundaries are hit exactly as in the FP64 kernel; far from the hole,
+ *    where the step is surely the cap, the step rule reads no radius root;
  *  - each ray's render constants live in registers (loaded when the ray is
  *    loaded), not re-read from the table every RHS.
  */
